@@ -1,0 +1,253 @@
+"""batchfit B200 backend: batched bounded Levenberg-Marquardt spectral fitting on
+NVIDIA B200 (sm_100a).
+
+``fit`` mirrors the reference Python API (python/batchfit/__init__.py:63-112):
+shared x[M], fit-major y[N,M], p0 [P] / [N,P] / None (data-only guesses on the
+GPU), bounds (lower, upper) as scalars or [P] (equal bounds fix a coordinate), and
+the same FitResult / FitResultWithUncertainties tuples, FitStatus and
+UncertaintyStatus codes.  Like the reference's explicit GPU device, results are
+float32 and an explicit CUDA request never falls back to the CPU.
+
+Inputs may be numpy arrays (host memory; the library pipelines the copies) or CUDA
+tensors exposing ``__cuda_array_interface__`` (device memory, zero copy; outputs
+are then torch CUDA tensors).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from enum import IntEnum
+from typing import NamedTuple
+
+import numpy as np
+
+from . import _capi
+
+__version__ = "0.1.0"
+__all__ = ["fit", "FitResult", "FitResultWithUncertainties", "FitStatus", "UncertaintyStatus", "cuda_available",
+           "MODELS", "__version__"]
+
+MODELS = {"gaussian": 0, "lorentzian": 1, "pseudo_voigt": 2, "two_lorentzian": 3}
+_PARAMETERS = {"gaussian": 3, "lorentzian": 3, "pseudo_voigt": 4, "two_lorentzian": 8}
+_POLICIES = {"reference": _capi.BF_POLICY_REFERENCE, "parity": _capi.BF_POLICY_PARITY}
+
+
+class FitStatus(IntEnum):
+    converged = 0
+    max_iterations = 1
+    singular_matrix = 2
+    invalid_input = 3
+    degenerate_data = 4
+    unresolved_peak = 5
+
+
+class UncertaintyStatus(IntEnum):
+    available = 0
+    not_converged = 1
+    insufficient_dof = 2
+    singular_matrix = 3
+    active_bound = 4
+    invalid_input = 5
+
+
+class FitResult(NamedTuple):
+    params: np.ndarray
+    status: np.ndarray
+    iterations: np.ndarray
+    chi2: np.ndarray
+
+
+class FitResultWithUncertainties(NamedTuple):
+    params: np.ndarray
+    status: np.ndarray
+    iterations: np.ndarray
+    chi2: np.ndarray
+    covariance: np.ndarray
+    stderr: np.ndarray
+    uncertainty_status: np.ndarray
+
+
+_contexts: dict[int, _capi.Context] = {}
+_contexts_lock = threading.Lock()
+
+
+def context(device: int = 0) -> _capi.Context:
+    """The process-wide context of a CUDA device (created on first use)."""
+    with _contexts_lock:
+        ctx = _contexts.get(device)
+        if ctx is None:
+            ctx = _capi.Context(device)
+            _contexts[device] = ctx
+        return ctx
+
+
+def cuda_available() -> bool:
+    """Whether the library loads and an sm_100-class device is present."""
+    return bool(_capi.load().bf_cuda_available())
+
+
+def _real_array(value, name):
+    array = np.asarray(value)
+    if array.dtype.kind not in "fiu":
+        raise TypeError(f"{name} must contain real numeric values")
+    return array
+
+
+def _is_device(value) -> bool:
+    return hasattr(value, "__cuda_array_interface__")
+
+
+def solver_options(model: str, bounds_lower, bounds_upper, policy: str = "parity", **overrides):
+    """bf_solver_options for `model`: the policy's defaults, the given bounds, and
+    any field overrides (max_iterations, initial_lambda, gradient_tolerance,
+    step_tolerance, cost_tolerance, scaled_cholesky, noise_floor, step_quantum)."""
+    if policy not in _POLICIES:
+        raise ValueError(f"policy must be one of {tuple(_POLICIES)}")
+    o = _capi.default_options(MODELS[model], _POLICIES[policy])
+    p = _PARAMETERS[model]
+    for k in range(p):
+        o.lower[k] = float(bounds_lower[k])
+        o.upper[k] = float(bounds_upper[k])
+    for key, value in overrides.items():
+        if not hasattr(o, key):
+            raise ValueError(f"unknown solver option {key!r}")
+        setattr(o, key, value)
+    return o
+
+
+def _bounds(bounds, p):
+    if bounds is None:
+        return np.full(p, -np.inf, np.float32), np.full(p, np.inf, np.float32)
+    if not isinstance(bounds, (tuple, list)) or len(bounds) != 2:
+        raise ValueError("bounds must be (lower, upper), each scalar or [P]")
+    lower, upper = (_real_array(value, "bounds") for value in bounds)
+    if lower.shape not in ((), (p,)) or upper.shape not in ((), (p,)):
+        raise ValueError(f"each bound must be scalar or have shape [{p}]")
+    maximum = np.finfo(np.float32).max
+    if any(np.any(np.isfinite(b) & (np.abs(b.astype(np.float64)) > maximum)) for b in (lower, upper)):
+        raise ValueError("finite bounds must be representable in the fitting dtype")
+    lower = np.ascontiguousarray(np.broadcast_to(lower, (p,)), dtype=np.float32)
+    upper = np.ascontiguousarray(np.broadcast_to(upper, (p,)), dtype=np.float32)
+    # python/bindings.cpp:264-273 rejects these before fitting.
+    if (np.any(np.isnan(lower)) or np.any(np.isnan(upper)) or np.any(lower > upper)
+            or np.any(lower == np.inf) or np.any(upper == -np.inf)):
+        raise ValueError("invalid parameter bounds")
+    return lower, upper
+
+
+def fit(x, y, model="lorentzian", p0=None, bounds=None, device="auto", *, uncertainties=False,
+        policy="parity", group_lanes=0, options=None):
+    """Fit shared x[M] and y[N,M]; return params[N,P], status/iterations/chi2[N].
+
+    A single y[M] is accepted as N=1.  ``device`` is "auto" or "cuda"; both run on
+    the GPU and never fall back.  ``policy`` selects the stopping rules: "parity"
+    (default) iterates to the float32 noise floor to match the float64 solution,
+    "reference" uses the reference float solver's tolerances.  ``options`` may be
+    a ready bf_solver_options (see ``solver_options``) and then overrides both.
+    """
+    if model not in _PARAMETERS:
+        raise ValueError(f"unknown model {model!r}; choose one of {tuple(_PARAMETERS)}")
+    if device not in ("auto", "cuda"):
+        raise ValueError("device must be 'auto' or 'cuda' (the CPU and Metal devices belong to the reference package)")
+    if not isinstance(uncertainties, (bool, np.bool_)):
+        raise TypeError("uncertainties must be a boolean")
+    if _is_device(x) or _is_device(y):
+        return _fit_device(x, y, model, p0, bounds, bool(uncertainties), policy, group_lanes, options)
+    x, y = _real_array(x, "x"), _real_array(y, "y")
+    if x.ndim != 1 or not x.size:
+        raise ValueError("x must have nonempty shape [M]")
+    if y.ndim == 1:
+        y = y.reshape(1, -1)
+    if y.ndim != 2 or y.shape[1] != x.size:
+        raise ValueError("y must have shape [N,M] matching x[M]")
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    n, p = y.shape[0], _PARAMETERS[model]
+    if p0 is not None:
+        p0 = _real_array(p0, "p0")
+        if p0.shape == (p,):
+            p0 = np.broadcast_to(p0, (n, p))
+        if p0.shape != (n, p):
+            raise ValueError(f"p0 must have shape [{p}] or [{n},{p}]")
+        p0 = np.ascontiguousarray(p0, dtype=np.float32)
+    lower, upper = _bounds(bounds, p)
+    opts = options if options is not None else solver_options(model, lower, upper, policy)
+    ctx = context(0)
+    params = np.empty((n, p), np.float32)
+    status = np.empty(n, np.int32)
+    iterations = np.empty(n, np.uint32)
+    chi2 = np.empty(n, np.float32)
+    cov = np.empty((n, p, p), np.float32) if uncertainties else None
+    se = np.empty((n, p), np.float32) if uncertainties else None
+    us = np.empty(n, np.int32) if uncertainties else None
+    ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    args = _capi.FitArgs(MODELS[model], n, x.size, ptr(x), ptr(y), ptr(p0), _capi.BF_MEMORY_HOST,
+                         int(bool(uncertainties)), int(group_lanes), opts)
+    outs = _capi.FitOutputs(ptr(params), ptr(status), ptr(iterations), ptr(chi2), ptr(cov), ptr(se), ptr(us))
+    ctx.fit(args, outs)
+    if uncertainties:
+        return FitResultWithUncertainties(params, status, iterations, chi2, cov, se, us)
+    return FitResult(params, status, iterations, chi2)
+
+
+def _fit_device(x, y, model, p0, bounds, uncertainties, policy, group_lanes, options):
+    import torch  # device-memory inputs come from torch (plumbing only)
+
+    if not (isinstance(x, torch.Tensor) and isinstance(y, torch.Tensor)):
+        raise TypeError("device inputs must be torch CUDA tensors")
+    if x.dtype != torch.float32 or y.dtype != torch.float32:
+        raise TypeError("device inputs must be float32")
+    if y.dim() == 1:
+        y = y.reshape(1, -1)
+    if x.dim() != 1 or x.numel() == 0 or y.dim() != 2 or y.shape[1] != x.numel():
+        raise ValueError("expected x[M] and y[N,M] with M>0")
+    if x.device != y.device:
+        raise ValueError("x and y must be on the same device")
+    x = x.contiguous()
+    y = y.contiguous()
+    n, p = y.shape[0], _PARAMETERS[model]
+    if p0 is not None:
+        p0 = torch.as_tensor(p0, dtype=torch.float32, device=y.device)
+        if p0.shape == (p,):
+            p0 = p0.expand(n, p)
+        if tuple(p0.shape) != (n, p):
+            raise ValueError(f"p0 must have shape [{p}] or [{n},{p}]")
+        p0 = p0.contiguous()
+    lower, upper = _bounds(bounds, p)
+    opts = options if options is not None else solver_options(model, lower, upper, policy)
+    device_index = y.device.index or 0
+    ctx = context(device_index)
+    kw = dict(device=y.device)
+    params = torch.empty((n, p), dtype=torch.float32, **kw)
+    status = torch.empty(n, dtype=torch.int32, **kw)
+    iterations = torch.empty(n, dtype=torch.int32, **kw)
+    chi2 = torch.empty(n, dtype=torch.float32, **kw)
+    cov = torch.empty((n, p, p), dtype=torch.float32, **kw) if uncertainties else None
+    se = torch.empty((n, p), dtype=torch.float32, **kw) if uncertainties else None
+    us = torch.empty(n, dtype=torch.int32, **kw) if uncertainties else None
+    ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())  # noqa: E731
+    args = _capi.FitArgs(MODELS[model], n, x.numel(), ptr(x), ptr(y), ptr(p0), _capi.BF_MEMORY_DEVICE,
+                         int(uncertainties), int(group_lanes), opts)
+    outs = _capi.FitOutputs(ptr(params), ptr(status), ptr(iterations), ptr(chi2), ptr(cov), ptr(se), ptr(us))
+    torch.cuda.current_stream(y.device).synchronize()
+    ctx.fit(args, outs)
+    if uncertainties:
+        return FitResultWithUncertainties(params, status, iterations, chi2, cov, se, us)
+    return FitResult(params, status, iterations, chi2)
+
+
+def guess(x, y, model="lorentzian"):
+    """Data-only initial guesses on the GPU -> (params[N,P], guess_status[N])."""
+    if model not in _PARAMETERS:
+        raise ValueError(f"unknown model {model!r}")
+    x = np.ascontiguousarray(_real_array(x, "x"), dtype=np.float32)
+    y = np.ascontiguousarray(_real_array(y, "y"), dtype=np.float32)
+    if y.ndim == 1:
+        y = y.reshape(1, -1)
+    n, p = y.shape[0], _PARAMETERS[model]
+    params = np.empty((n, p), np.float32)
+    status = np.empty(n, np.int32)
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    context(0).guess(MODELS[model], n, x.size, ptr(x), ptr(y), _capi.BF_MEMORY_HOST, ptr(params), ptr(status))
+    return params, status

@@ -1,0 +1,636 @@
+// Host runtime and C ABI of the batchfit B200 backend (include/batchfit_cuda.h).
+//
+// A context owns one device, two streams, reusable device staging buffers and the
+// per-stream work counters of the persistent kernels.  Device-memory calls launch
+// one kernel over all fits.  Host-memory calls run a chunked pipeline: chunk c is
+// copied in, fitted and copied out on stream c % 2, so the copies of one chunk
+// overlap the kernel of the other.
+#include "batchfit_cuda.h"
+#include "bf_kernels.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &message) {
+    g_last_error = message;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(BF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define BF_CUDA(call)                                                                              \
+    do {                                                                                           \
+        const cudaError_t bf_e = (call);                                                           \
+        if (bf_e != cudaSuccess)                                                                   \
+            return cuda_fail(bf_e, #call);                                                         \
+    } while (0)
+
+int parameter_count(int model) { return model == 2 ? 4 : model == 3 ? 8 : 3; }
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t need) {
+        if (need <= bytes)
+            return cudaSuccess;
+        if (ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        const cudaError_t e = cudaMalloc(&ptr, need);
+        if (e == cudaSuccess)
+            bytes = need;
+        return e;
+    }
+    void release() {
+        if (ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+// Device-side storage of one in-flight chunk.
+struct Slot {
+    DeviceBuffer y, p0, params, status, iterations, chi2, cov, se, ustatus, counter;
+    cudaEvent_t k0 = nullptr, k1 = nullptr;
+};
+
+constexpr int kSlots = 2;
+
+} // namespace
+
+struct bf_cuda_context {
+    int device = 0;
+    int sms = 0;
+    std::mutex mutex;
+    std::atomic<bool> busy{false};
+    cudaStream_t stream[kSlots] = {nullptr, nullptr};
+    cudaEvent_t start = nullptr, stop = nullptr, joined = nullptr;
+    DeviceBuffer x;
+    Slot slot[kSlots];
+    bf_cuda_timing last{};
+    // Kernel-event pairs of the in-flight submission (one per chunk).
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kernel_events;
+    std::vector<cudaEvent_t> event_pool;
+    int launches = 0;
+    int lanes = 0;
+    bf::LaunchInfo info{};
+};
+
+struct bf_cuda_pending {
+    bf_cuda_context *ctx;
+    int result;
+};
+
+namespace {
+
+constexpr int kSmemLimit = 227 * 1024;
+
+int choose_lanes(int model, uint32_t m, int requested) {
+    int lanes = requested;
+    if (lanes != 8 && lanes != 16 && lanes != 32) {
+        // Points per lane between ~8 and ~32 keeps the group reduction and the FP64
+        // control amortised without starving the scheduler of independent fits.
+        lanes = m <= 192 ? 8 : m <= 768 ? 16 : 32;
+    }
+    // Fewer, wider groups per CTA when the per-group spectrum buffers do not fit.
+    while (lanes < 32 && bf::smem_bytes(model, lanes, int(m)) > kSmemLimit)
+        lanes *= 2;
+    return lanes;
+}
+
+bool options_valid(const bf_solver_options &o, int p) {
+    if (!std::isfinite(o.initial_lambda) || o.initial_lambda <= 0.0)
+        return false;
+    for (double t : {o.gradient_tolerance, o.step_tolerance, o.cost_tolerance})
+        if (!std::isfinite(t) || t < 0.0)
+            return false;
+    for (int k = 0; k < p; ++k) {
+        const float lo = o.lower[k], hi = o.upper[k];
+        if (std::isnan(lo) || std::isnan(hi) || lo > hi || lo == std::numeric_limits<float>::infinity() ||
+            hi == -std::numeric_limits<float>::infinity())
+            return false;
+    }
+    return true;
+}
+
+bf::FitArgs make_args(const bf_fit_args &in, int p) {
+    bf::FitArgs a{};
+    const bf_solver_options &o = in.options;
+    a.m = int(in.m);
+    a.uncertainties = in.uncertainties ? 1 : 0;
+    a.max_iterations = o.max_iterations;
+    a.flags = (o.compensated_sum ? bf::kFlagCompensated : 0u) | (o.scaled_cholesky ? bf::kFlagScaledCholesky : 0u);
+    a.policy = o.policy == BF_POLICY_PARITY ? bf::kPolicyParity : bf::kPolicyReference;
+    a.options_ok = options_valid(o, p) ? 1u : 0u;
+    if (a.policy == bf::kPolicyReference) {
+        // The reference float solver holds lambda and tolerances as float.
+        a.lambda0 = double(float(o.initial_lambda));
+        a.gtol = double(float(o.gradient_tolerance));
+        a.xtol = double(float(o.step_tolerance));
+        a.ftol = double(float(o.cost_tolerance));
+    } else {
+        a.lambda0 = o.initial_lambda;
+        a.gtol = o.gradient_tolerance;
+        a.xtol = o.step_tolerance;
+        a.ftol = o.cost_tolerance;
+    }
+    a.noise_floor = o.noise_floor;
+    a.step_quantum = o.step_quantum;
+    for (int k = 0; k < 8; ++k) {
+        a.lower[k] = k < p ? o.lower[k] : -std::numeric_limits<float>::infinity();
+        a.upper[k] = k < p ? o.upper[k] : std::numeric_limits<float>::infinity();
+    }
+    return a;
+}
+
+int validate(const bf_fit_args *args, const bf_fit_outputs *out) {
+    if (!args || !out)
+        return fail(BF_ERR_INVALID_ARGUMENT, "null argument block");
+    if (args->model < 0 || args->model > 3)
+        return fail(BF_ERR_INVALID_ARGUMENT, "unknown model id");
+    if (args->m == 0)
+        return fail(BF_ERR_INVALID_ARGUMENT, "fit requires nonempty x[M] (M > 0)");
+    if (args->memory != BF_MEMORY_HOST && args->memory != BF_MEMORY_DEVICE)
+        return fail(BF_ERR_INVALID_ARGUMENT, "memory must be BF_MEMORY_HOST or BF_MEMORY_DEVICE");
+    const uint32_t limit = uint32_t(bf::max_points(args->model));
+    if (args->m > limit)
+        return fail(BF_ERR_INVALID_ARGUMENT,
+                    "M=" + std::to_string(args->m) + " exceeds this backend's limit of " + std::to_string(limit));
+    const int p = parameter_count(args->model);
+    if (args->n > uint64_t(std::numeric_limits<int64_t>::max()) / (uint64_t(args->m) + uint64_t(p) * p))
+        return fail(BF_ERR_INVALID_ARGUMENT, "N*M or N*P*P overflows 64-bit indexing");
+    if (args->group_lanes != 0 && args->group_lanes != 8 && args->group_lanes != 16 && args->group_lanes != 32)
+        return fail(BF_ERR_INVALID_ARGUMENT, "group_lanes must be 0, 8, 16 or 32");
+    if (args->n == 0)
+        return BF_OK;
+    if (!args->x || !args->y)
+        return fail(BF_ERR_INVALID_ARGUMENT, "x and y are required");
+    if (!out->params || !out->status || !out->iterations || !out->chi2)
+        return fail(BF_ERR_INVALID_ARGUMENT, "params, status, iterations and chi2 outputs are required");
+    if (args->uncertainties && (!out->covariance || !out->standard_errors || !out->uncertainty_status))
+        return fail(BF_ERR_INVALID_ARGUMENT, "uncertainty outputs are required when uncertainties is set");
+    return BF_OK;
+}
+
+cudaEvent_t take_event(bf_cuda_context *ctx) {
+    if (!ctx->event_pool.empty()) {
+        cudaEvent_t e = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Enqueue a whole fit on the context's streams.  Returns BF_OK once queued.
+int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &out, const bf::GuessArgs &guess_args) {
+    const int p = parameter_count(in.model);
+    const uint64_t n = in.n, m = in.m;
+    const int lanes = choose_lanes(in.model, in.m, in.group_lanes);
+    ctx->lanes = lanes;
+    ctx->launches = 0;
+    for (auto &ev : ctx->kernel_events) {
+        ctx->event_pool.push_back(ev.first);
+        ctx->event_pool.push_back(ev.second);
+    }
+    ctx->kernel_events.clear();
+    BF_CUDA(cudaSetDevice(ctx->device));
+    BF_CUDA(cudaEventRecord(ctx->start, ctx->stream[0]));
+    BF_CUDA(cudaStreamWaitEvent(ctx->stream[1], ctx->start, 0));
+    bf::FitArgs base = make_args(in, p);
+
+    if (in.memory == BF_MEMORY_DEVICE) {
+        Slot &s = ctx->slot[0];
+        BF_CUDA(s.counter.reserve(sizeof(unsigned long long)));
+        bf::FitArgs a = base;
+        a.x = in.x;
+        a.y = in.y;
+        a.p0 = in.p0;
+        a.params = out.params;
+        a.status = out.status;
+        a.iterations = out.iterations;
+        a.chi2 = out.chi2;
+        a.covariance = out.covariance;
+        a.stderr_out = out.standard_errors;
+        a.ustatus = out.uncertainty_status;
+        a.n = (long long)n;
+        a.work_counter = static_cast<unsigned long long *>(s.counter.ptr);
+        if (n > 0) {
+            BF_CUDA(cudaMemsetAsync(a.work_counter, 0, sizeof(unsigned long long), ctx->stream[0]));
+            cudaEvent_t k0 = take_event(ctx), k1 = take_event(ctx);
+            BF_CUDA(cudaEventRecord(k0, ctx->stream[0]));
+            BF_CUDA(bf::launch_fit(in.model, lanes, a, guess_args, ctx->sms, ctx->stream[0], &ctx->info));
+            BF_CUDA(cudaEventRecord(k1, ctx->stream[0]));
+            ctx->kernel_events.push_back({k0, k1});
+            ctx->launches = 1;
+        }
+        BF_CUDA(cudaEventRecord(ctx->stop, ctx->stream[0]));
+        return BF_OK;
+    }
+
+    // Host memory: x once, then double-buffered chunks.
+    BF_CUDA(ctx->x.reserve(m * sizeof(float)));
+    BF_CUDA(cudaMemcpyAsync(ctx->x.ptr, in.x, m * sizeof(float), cudaMemcpyHostToDevice, ctx->stream[0]));
+    cudaEvent_t x_ready = take_event(ctx);
+    BF_CUDA(cudaEventRecord(x_ready, ctx->stream[0]));
+    BF_CUDA(cudaStreamWaitEvent(ctx->stream[1], x_ready, 0));
+    ctx->event_pool.push_back(x_ready);
+    // ~128 MB of observations per chunk, at least a few waves of fits.
+    uint64_t chunk = std::max<uint64_t>(16384, (128ull << 20) / (m * sizeof(float)));
+    if (chunk > n)
+        chunk = n;
+    const bool has_p0 = in.p0 != nullptr;
+    for (int i = 0; i < kSlots && n > 0; ++i) {
+        Slot &s = ctx->slot[i];
+        BF_CUDA(s.y.reserve(chunk * m * sizeof(float)));
+        if (has_p0)
+            BF_CUDA(s.p0.reserve(chunk * p * sizeof(float)));
+        BF_CUDA(s.params.reserve(chunk * p * sizeof(float)));
+        BF_CUDA(s.status.reserve(chunk * sizeof(int32_t)));
+        BF_CUDA(s.iterations.reserve(chunk * sizeof(uint32_t)));
+        BF_CUDA(s.chi2.reserve(chunk * sizeof(float)));
+        if (in.uncertainties) {
+            BF_CUDA(s.cov.reserve(chunk * p * p * sizeof(float)));
+            BF_CUDA(s.se.reserve(chunk * p * sizeof(float)));
+            BF_CUDA(s.ustatus.reserve(chunk * sizeof(int32_t)));
+        }
+        BF_CUDA(s.counter.reserve(sizeof(unsigned long long)));
+    }
+    int c = 0;
+    for (uint64_t first = 0; first < n; first += chunk, ++c) {
+        const uint64_t count = std::min(chunk, n - first);
+        Slot &s = ctx->slot[c % kSlots];
+        cudaStream_t st = ctx->stream[c % kSlots];
+        BF_CUDA(cudaMemcpyAsync(s.y.ptr, in.y + first * m, count * m * sizeof(float), cudaMemcpyHostToDevice, st));
+        if (has_p0)
+            BF_CUDA(cudaMemcpyAsync(s.p0.ptr, in.p0 + first * p, count * p * sizeof(float), cudaMemcpyHostToDevice,
+                                    st));
+        bf::FitArgs a = base;
+        a.x = static_cast<const float *>(ctx->x.ptr);
+        a.y = static_cast<const float *>(s.y.ptr);
+        a.p0 = has_p0 ? static_cast<const float *>(s.p0.ptr) : nullptr;
+        a.params = static_cast<float *>(s.params.ptr);
+        a.status = static_cast<int32_t *>(s.status.ptr);
+        a.iterations = static_cast<uint32_t *>(s.iterations.ptr);
+        a.chi2 = static_cast<float *>(s.chi2.ptr);
+        a.covariance = static_cast<float *>(s.cov.ptr);
+        a.stderr_out = static_cast<float *>(s.se.ptr);
+        a.ustatus = static_cast<int32_t *>(s.ustatus.ptr);
+        a.n = (long long)count;
+        a.work_counter = static_cast<unsigned long long *>(s.counter.ptr);
+        BF_CUDA(cudaMemsetAsync(a.work_counter, 0, sizeof(unsigned long long), st));
+        cudaEvent_t k0 = take_event(ctx), k1 = take_event(ctx);
+        BF_CUDA(cudaEventRecord(k0, st));
+        BF_CUDA(bf::launch_fit(in.model, lanes, a, guess_args, ctx->sms, st, &ctx->info));
+        BF_CUDA(cudaEventRecord(k1, st));
+        ctx->kernel_events.push_back({k0, k1});
+        ++ctx->launches;
+        auto d2h = [&](void *dst, const void *src, size_t bytes) {
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+        };
+        BF_CUDA(d2h(out.params + first * p, s.params.ptr, count * p * sizeof(float)));
+        BF_CUDA(d2h(out.status + first, s.status.ptr, count * sizeof(int32_t)));
+        BF_CUDA(d2h(out.iterations + first, s.iterations.ptr, count * sizeof(uint32_t)));
+        BF_CUDA(d2h(out.chi2 + first, s.chi2.ptr, count * sizeof(float)));
+        if (in.uncertainties) {
+            BF_CUDA(d2h(out.covariance + first * p * p, s.cov.ptr, count * p * p * sizeof(float)));
+            BF_CUDA(d2h(out.standard_errors + first * p, s.se.ptr, count * p * sizeof(float)));
+            BF_CUDA(d2h(out.uncertainty_status + first, s.ustatus.ptr, count * sizeof(int32_t)));
+        }
+    }
+    BF_CUDA(cudaEventRecord(ctx->joined, ctx->stream[1]));
+    BF_CUDA(cudaStreamWaitEvent(ctx->stream[0], ctx->joined, 0));
+    BF_CUDA(cudaEventRecord(ctx->stop, ctx->stream[0]));
+    return BF_OK;
+}
+
+int finish(bf_cuda_context *ctx) {
+    BF_CUDA(cudaEventSynchronize(ctx->stop));
+    float total = 0.0f;
+    BF_CUDA(cudaEventElapsedTime(&total, ctx->start, ctx->stop));
+    double kernel = 0.0;
+    for (auto &ev : ctx->kernel_events) {
+        float t = 0.0f;
+        BF_CUDA(cudaEventElapsedTime(&t, ev.first, ev.second));
+        kernel += t;
+    }
+    ctx->last.kernel_ms = kernel;
+    ctx->last.total_ms = total;
+    ctx->last.launches = uint32_t(ctx->launches);
+    ctx->last.group_lanes = ctx->lanes;
+    ctx->last.grid = ctx->info.grid;
+    ctx->last.blocks_per_sm = ctx->info.blocks_per_sm;
+    return BF_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *bf_cuda_last_error(void) { return g_last_error.c_str(); }
+
+int bf_cuda_version(void) { return 10; }
+
+int bf_cuda_available(void) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return 0;
+    }
+    for (int d = 0; d < count; ++d) {
+        cudaDeviceProp prop{};
+        if (cudaGetDeviceProperties(&prop, d) == cudaSuccess && prop.major == 10)
+            return 1;
+    }
+    return 0;
+}
+
+uint32_t bf_cuda_max_points(int32_t model) {
+    if (model < 0 || model > 3)
+        return 0;
+    return uint32_t(bf::max_points(model));
+}
+
+int bf_cuda_context_create(int device, bf_cuda_context **out) {
+    if (!out)
+        return fail(BF_ERR_INVALID_ARGUMENT, "null output pointer");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(BF_ERR_UNAVAILABLE, "CUDA fitting is unavailable: no CUDA device");
+    }
+    if (device < 0 || device >= count)
+        return fail(BF_ERR_INVALID_ARGUMENT, "device index out of range");
+    cudaDeviceProp prop{};
+    BF_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+        return fail(BF_ERR_UNAVAILABLE, std::string("CUDA fitting is unavailable: device '") + prop.name +
+                                            "' is not sm_100 (this build targets sm_100a only)");
+    auto *ctx = new bf_cuda_context();
+    ctx->device = device;
+    ctx->sms = prop.multiProcessorCount;
+    cudaError_t e = cudaSetDevice(device);
+    for (int i = 0; i < kSlots && e == cudaSuccess; ++i)
+        e = cudaStreamCreateWithFlags(&ctx->stream[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&ctx->start);
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&ctx->stop);
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&ctx->joined);
+    if (e != cudaSuccess) {
+        bf_cuda_context_destroy(ctx);
+        return cuda_fail(e, "context setup");
+    }
+    *out = ctx;
+    return BF_OK;
+}
+
+void bf_cuda_context_destroy(bf_cuda_context *ctx) {
+    if (!ctx)
+        return;
+    cudaSetDevice(ctx->device);
+    for (auto &st : ctx->stream)
+        if (st)
+            cudaStreamSynchronize(st);
+    for (auto &s : ctx->slot) {
+        s.y.release();
+        s.p0.release();
+        s.params.release();
+        s.status.release();
+        s.iterations.release();
+        s.chi2.release();
+        s.cov.release();
+        s.se.release();
+        s.ustatus.release();
+        s.counter.release();
+    }
+    ctx->x.release();
+    for (auto &ev : ctx->kernel_events) {
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+    for (auto ev : ctx->event_pool)
+        cudaEventDestroy(ev);
+    for (cudaEvent_t ev : {ctx->start, ctx->stop, ctx->joined})
+        if (ev)
+            cudaEventDestroy(ev);
+    for (auto &st : ctx->stream)
+        if (st)
+            cudaStreamDestroy(st);
+    delete ctx;
+}
+
+int bf_cuda_default_options(int32_t model, uint32_t policy, bf_solver_options *out) {
+    if (!out)
+        return fail(BF_ERR_INVALID_ARGUMENT, "null output pointer");
+    if (model < 0 || model > 3)
+        return fail(BF_ERR_INVALID_ARGUMENT, "unknown model id");
+    if (policy != BF_POLICY_REFERENCE && policy != BF_POLICY_PARITY)
+        return fail(BF_ERR_INVALID_ARGUMENT, "unknown policy");
+    bf_solver_options o{};
+    o.max_iterations = 100;
+    o.initial_lambda = 1e-3;
+    // Float defaults (solver.hpp:29-31) for the reference policy, double defaults
+    // for the parity policy.
+    o.gradient_tolerance = policy == BF_POLICY_PARITY ? 1e-10 : 1e-5;
+    o.step_tolerance = policy == BF_POLICY_PARITY ? 1e-10 : 1e-6;
+    o.cost_tolerance = policy == BF_POLICY_PARITY ? 1e-12 : 1e-6;
+    o.compensated_sum = 1;
+    o.scaled_cholesky = 0;
+    o.policy = policy;
+    o.noise_floor = 16.0;
+    o.step_quantum = 16.0;
+    for (int k = 0; k < 8; ++k) {
+        o.lower[k] = -std::numeric_limits<float>::infinity();
+        o.upper[k] = std::numeric_limits<float>::infinity();
+    }
+    *out = o;
+    return BF_OK;
+}
+
+int bf_cuda_submit(bf_cuda_context *ctx, const bf_fit_args *args, const bf_fit_outputs *out,
+                   bf_cuda_pending **pending) {
+    if (!ctx || !pending)
+        return fail(BF_ERR_INVALID_ARGUMENT, "null context or pending pointer");
+    *pending = nullptr;
+    int rc = validate(args, out);
+    if (rc != BF_OK)
+        return rc;
+    if (ctx->busy.exchange(true))
+        return fail(BF_ERR_BUSY, "a submission is already in flight on this context");
+    {
+        std::lock_guard<std::mutex> lock(ctx->mutex);
+        rc = enqueue(ctx, *args, *out, bf::GuessArgs{nullptr, nullptr, 0});
+    }
+    if (rc != BF_OK) {
+        // Drain whatever was queued before the failure.
+        for (auto &st : ctx->stream)
+            cudaStreamSynchronize(st);
+        ctx->busy.store(false);
+        return rc;
+    }
+    *pending = new bf_cuda_pending{ctx, BF_OK};
+    return BF_OK;
+}
+
+int bf_cuda_ready(bf_cuda_pending *pending) {
+    if (!pending)
+        return -BF_ERR_INVALID_ARGUMENT;
+    const cudaError_t e = cudaEventQuery(pending->ctx->stop);
+    if (e == cudaSuccess)
+        return 1;
+    if (e == cudaErrorNotReady)
+        return 0;
+    cuda_fail(e, "cudaEventQuery");
+    return -BF_ERR_CUDA;
+}
+
+int bf_cuda_wait(bf_cuda_pending *pending) {
+    if (!pending)
+        return fail(BF_ERR_INVALID_ARGUMENT, "null pending handle");
+    bf_cuda_context *ctx = pending->ctx;
+    int rc;
+    {
+        std::lock_guard<std::mutex> lock(ctx->mutex);
+        rc = finish(ctx);
+        if (rc == BF_OK) {
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess)
+                rc = cuda_fail(e, "fit kernel");
+        }
+    }
+    ctx->busy.store(false);
+    delete pending;
+    return rc;
+}
+
+int bf_cuda_fit(bf_cuda_context *ctx, const bf_fit_args *args, const bf_fit_outputs *out) {
+    bf_cuda_pending *pending = nullptr;
+    const int rc = bf_cuda_submit(ctx, args, out, &pending);
+    if (rc != BF_OK)
+        return rc;
+    return bf_cuda_wait(pending);
+}
+
+int bf_cuda_guess(bf_cuda_context *ctx, int32_t model, uint64_t n, uint32_t m, const float *x, const float *y,
+                  int32_t memory, float *params, int32_t *guess_status) {
+    if (!ctx)
+        return fail(BF_ERR_INVALID_ARGUMENT, "null context");
+    bf_fit_args args{};
+    args.model = model;
+    args.n = n;
+    args.m = m;
+    args.x = x;
+    args.y = y;
+    args.memory = memory;
+    bf_cuda_default_options(model < 0 || model > 3 ? 0 : model, BF_POLICY_REFERENCE, &args.options);
+    // The guess-only launch writes no fit outputs; validation needs placeholders.
+    float dummy_f = 0.0f;
+    int32_t dummy_i = 0;
+    uint32_t dummy_u = 0;
+    bf_fit_outputs out{&dummy_f, &dummy_i, &dummy_u, &dummy_f, nullptr, nullptr, nullptr};
+    int rc = validate(&args, &out);
+    if (rc != BF_OK)
+        return rc;
+    if (n > 0 && (!params || !guess_status))
+        return fail(BF_ERR_INVALID_ARGUMENT, "params and guess_status outputs are required");
+    if (ctx->busy.exchange(true))
+        return fail(BF_ERR_BUSY, "a submission is already in flight on this context");
+    std::lock_guard<std::mutex> lock(ctx->mutex);
+    const int p = parameter_count(model);
+    rc = BF_OK;
+    do {
+        if (n == 0)
+            break;
+        if (memory == BF_MEMORY_DEVICE) {
+            bf_fit_args a = args;
+            rc = enqueue(ctx, a, out, bf::GuessArgs{params, guess_status, 1});
+            if (rc == BF_OK)
+                rc = finish(ctx);
+            break;
+        }
+        // Host memory: stage everything on the device once (guesses are cheap).
+        DeviceBuffer dx, dy, dp, ds;
+        cudaError_t e = cudaSetDevice(ctx->device);
+        if (e == cudaSuccess)
+            e = dx.reserve(size_t(m) * sizeof(float));
+        if (e == cudaSuccess)
+            e = dy.reserve(size_t(n) * m * sizeof(float));
+        if (e == cudaSuccess)
+            e = dp.reserve(size_t(n) * p * sizeof(float));
+        if (e == cudaSuccess)
+            e = ds.reserve(size_t(n) * sizeof(int32_t));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(dx.ptr, x, size_t(m) * sizeof(float), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(dy.ptr, y, size_t(n) * m * sizeof(float), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(e, "guess staging");
+        } else {
+            bf_fit_args a = args;
+            a.x = static_cast<const float *>(dx.ptr);
+            a.y = static_cast<const float *>(dy.ptr);
+            a.memory = BF_MEMORY_DEVICE;
+            rc = enqueue(ctx, a, out,
+                         bf::GuessArgs{static_cast<float *>(dp.ptr), static_cast<int32_t *>(ds.ptr), 1});
+            if (rc == BF_OK)
+                rc = finish(ctx);
+            if (rc == BF_OK) {
+                e = cudaMemcpy(params, dp.ptr, size_t(n) * p * sizeof(float), cudaMemcpyDeviceToHost);
+                if (e == cudaSuccess)
+                    e = cudaMemcpy(guess_status, ds.ptr, size_t(n) * sizeof(int32_t), cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess)
+                    rc = cuda_fail(e, "guess readback");
+            }
+        }
+        dx.release();
+        dy.release();
+        dp.release();
+        ds.release();
+    } while (false);
+    ctx->busy.store(false);
+    return rc;
+}
+
+int bf_cuda_last_timing(bf_cuda_context *ctx, bf_cuda_timing *out) {
+    if (!ctx || !out)
+        return fail(BF_ERR_INVALID_ARGUMENT, "null argument");
+    *out = ctx->last;
+    return BF_OK;
+}
+
+int bf_cuda_host_alloc(size_t bytes, void **out) {
+    if (!out)
+        return fail(BF_ERR_INVALID_ARGUMENT, "null output pointer");
+    *out = nullptr;
+    if (bytes == 0)
+        return BF_OK;
+    BF_CUDA(cudaHostAlloc(out, bytes, cudaHostAllocPortable));
+    return BF_OK;
+}
+
+int bf_cuda_host_free(void *ptr) {
+    if (ptr)
+        BF_CUDA(cudaFreeHost(ptr));
+    return BF_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,409 @@
+// Data-only initial guess on the device, one thread group per spectrum.
+//
+// Restates initial_guess<float,Model> (include/batchfit/cpu/initial_guess.hpp:120-249)
+// with group-parallel searches, and rounds every operation exactly as the
+// reference's float C++ does (the _rn intrinsics: no contraction).  Its outputs
+// and status equal the reference's float guess bit for bit; the parallel searches
+// keep the reference's tie rules (first maximum / first minimum in index order).
+#pragma once
+
+#include "bf_device.cuh"
+#include "bf_models.cuh"
+
+namespace bf {
+
+enum GuessStatus : int { kGuessSuccess = 0, kGuessInvalid = 1, kGuessNoPeak = 2, kGuessInsufficient = 3 };
+
+// Values derived from the shared x grid, computed once per CTA.
+struct XConst {
+    int m;
+    int x_finite;        // every x finite (solver.hpp:223-226)
+    int varied_x;        // some x differs from x[0] (solver.hpp:238-239)
+    float spacing;       // detail::grid_spacing (solver.hpp:58-69)
+    int guess_ok;        // M>=5, finite, strictly increasing, finite span (initial_guess.hpp:131-141)
+    float guess_spacing; // min x[j]-x[j-1] (initial_guess.hpp:133-139)
+    int count;           // max(1, M/10) edge samples per side (initial_guess.hpp:142)
+    int n1;              // power of two >= count (sorting width per side)
+    float left_x, right_x; // edge-median abscissae (initial_guess.hpp:151-153)
+};
+
+// Ascending bitonic sort of `batches` consecutive arrays of n (power of two) floats.
+template <int G>
+__device__ __forceinline__ void bitonic_sort(const Group<G> &g, float *buf, int n, int batches) {
+    const int pairs = (n >> 1) * batches;
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int t = int(g.lane); t < pairs; t += G) {
+                const int b = t / (n >> 1), u = t % (n >> 1);
+                const int i = ((u & ~(j - 1)) << 1) | (u & (j - 1));
+                float *a = buf + b * n;
+                const float lo = a[i], hi = a[i | j];
+                const bool ascending = (i & k) == 0;
+                if (ascending ? (lo > hi) : (lo < hi)) {
+                    a[i] = hi;
+                    a[i | j] = lo;
+                }
+            }
+            g.sync();
+        }
+    }
+}
+
+// Sort a bitonic sequence of n (power of two) floats ascending.
+template <int G> __device__ __forceinline__ void bitonic_merge(const Group<G> &g, float *buf, int n) {
+    for (int j = n >> 1; j > 0; j >>= 1) {
+        for (int t = int(g.lane); t < (n >> 1); t += G) {
+            const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+            const float lo = buf[i], hi = buf[i | j];
+            if (lo > hi) {
+                buf[i] = hi;
+                buf[i | j] = lo;
+            }
+        }
+        g.sync();
+    }
+}
+
+// detail::median on sorted values (initial_guess.hpp:25-30).
+__device__ __forceinline__ float sorted_median(const float *a, int n) {
+    return (n & 1) ? a[n / 2] : midpoint_rn(a[n / 2 - 1], a[n / 2]);
+}
+
+template <int MODEL> struct Signal {
+    // signal[j] = y[j] - (level + slope*(x[j]-left_x))   (initial_guess.hpp:158-162)
+    const float *xs, *ys;
+    float level, slope, left_x;
+    int m;
+    __device__ __forceinline__ float at(int j) const {
+        if constexpr (Model<MODEL>::paired)
+            return rsub(ys[j], radd(level, rmul(slope, rsub(xs[j], left_x))));
+        else
+            return rsub(ys[j], level); // slope == 0: equal value (up to the sign of zero)
+    }
+    // detail::smooth (initial_guess.hpp:32-36).
+    __device__ __forceinline__ float smooth(int j) const {
+        if (j == 0 || j + 1 == m)
+            return at(j);
+        return radd(radd(rmul(0.25f, at(j - 1)), rmul(0.5f, at(j))), rmul(0.25f, at(j + 1)));
+    }
+    // detail::raw_maximum (initial_guess.hpp:111-115): first max of s[j-1..j+1].
+    __device__ __forceinline__ int raw_maximum(int j) const {
+        int best = j - 1;
+        float bv = at(j - 1);
+        const float v0 = at(j), v1 = at(j + 1);
+        if (bv < v0) {
+            best = j;
+            bv = v0;
+        }
+        if (bv < v1)
+            best = j + 1;
+        return best;
+    }
+};
+
+// Group argmax of (value, index): larger value wins, ties go to the smaller index.
+template <int G> __device__ __forceinline__ void argmax_pair(const Group<G> &g, float &v, int &i) {
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1) {
+        const float ov = g.xor_(v, o);
+        const int oi = g.xor_(i, o);
+        if (ov > v || (ov == v && oi < i)) {
+            v = ov;
+            i = oi;
+        }
+    }
+}
+
+struct PeakFeature {
+    float amplitude, center, width, left_radius, right_radius;
+    bool valid;
+};
+
+// detail::peak (initial_guess.hpp:61-109) with the half-height walks done as
+// group-parallel searches for the nearest sample at or below half height.
+template <int MODEL, int G>
+__device__ PeakFeature find_peak(const Group<G> &g, const Signal<MODEL> &s, const float *xs, int index,
+                                 int begin, int end, bool mirror) {
+    PeakFeature r{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, false};
+    r.amplitude = s.at(index);
+    if (!(r.amplitude > 0.0f))
+        return r;
+    const float half = rdiv(r.amplitude, 2.0f);
+    // while (left > begin && signal[left] > half) --left;
+    int left = begin;
+    for (int top = index - 1; top >= begin; top -= G) {
+        const int pos = top - int(g.lane);
+        const bool hit = pos >= begin && s.at(pos) <= half;
+        const unsigned b = g.ballot(hit);
+        if (b) {
+            left = top - (__ffs(b) - 1);
+            break;
+        }
+    }
+    if (index == begin)
+        left = index;
+    // while (right < end && signal[right] > half) ++right;
+    int right = end;
+    for (int bot = index + 1; bot <= end; bot += G) {
+        const int pos = bot + int(g.lane);
+        const bool hit = pos <= end && s.at(pos) <= half;
+        const unsigned b = g.ballot(hit);
+        if (b) {
+            right = bot + (__ffs(b) - 1);
+            break;
+        }
+    }
+    if (index == end)
+        right = index;
+    const bool has_left = s.at(left) <= half, has_right = s.at(right) <= half;
+    if ((!has_left && (!mirror || begin == 0)) || (!has_right && (!mirror || end + 1 == s.m)) ||
+        (!has_left && !has_right))
+        return r;
+    int low = index > 2 ? index - 2 : 0;
+    int high = index + 2 < end ? index + 2 : end;
+    const int low_limit = has_left ? left + 1 : begin;
+    const int high_limit = has_right ? right - 1 : end;
+    low = low < low_limit ? low_limit : low;
+    high = high_limit < high ? high_limit : high;
+    float total = 0.0f;
+    r.center = xs[index];
+    for (int j = low; j <= high; ++j) {
+        const float w = rdiv(smax(0.0f, s.at(j)), r.amplitude);
+        if (w > 0.0f) {
+            total = radd(total, w);
+            r.center = lerp_rn(r.center, xs[j], rdiv(w, total));
+        }
+    }
+    auto crossing = [&](int a, int b) {
+        const float den = rsub(s.at(b), s.at(a));
+        if (!isfinite(den) || den == 0.0f)
+            return __int_as_float(0x7fffffff);
+        return lerp_rn(xs[a], xs[b], rdiv(rsub(half, s.at(a)), den));
+    };
+    if (has_left)
+        r.left_radius = rsub(r.center, crossing(left, left + 1));
+    if (has_right)
+        r.right_radius = rsub(crossing(right - 1, right), r.center);
+    if (!has_left)
+        r.left_radius = r.right_radius;
+    if (!has_right)
+        r.right_radius = r.left_radius;
+    r.width = radd(r.left_radius, r.right_radius);
+    r.valid = isfinite(r.center) && isfinite(r.width) && r.left_radius > 0.0f && r.right_radius > 0.0f;
+    return r;
+}
+
+// detail::prominence (initial_guess.hpp:38-54): walk outwards while the smoothed
+// signal stays at or below the start height, tracking the minimum on each side.
+template <int MODEL, int G>
+__device__ float prominence(const Group<G> &g, const Signal<MODEL> &s, int index) {
+    const float height = s.smooth(index);
+    float left = height, right = height;
+    for (int top = index - 1; top >= 0; top -= G) {
+        const int pos = top - int(g.lane);
+        const float v = pos >= 0 ? s.smooth(pos) : height;
+        const unsigned b = g.ballot(pos >= 0 && v > height);
+        const int stop = b ? __ffs(b) - 1 : G;
+        float mv = (int(g.lane) < stop && pos >= 0) ? v : height;
+#pragma unroll
+        for (int o = G / 2; o >= 1; o >>= 1)
+            mv = fminf(mv, g.xor_(mv, o));
+        left = smin(left, mv);
+        if (b)
+            break;
+    }
+    for (int bot = index + 1; bot < s.m; bot += G) {
+        const int pos = bot + int(g.lane);
+        const float v = pos < s.m ? s.smooth(pos) : height;
+        const unsigned b = g.ballot(pos < s.m && v > height);
+        const int stop = b ? __ffs(b) - 1 : G;
+        float mv = (int(g.lane) < stop && pos < s.m) ? v : height;
+#pragma unroll
+        for (int o = G / 2; o >= 1; o >>= 1)
+            mv = fminf(mv, g.xor_(mv, o));
+        right = smin(right, mv);
+        if (b)
+            break;
+    }
+    return rsub(height, smax(left, right));
+}
+
+// initial_guess<float,Model> for the spectrum ys[0..m).  `scratch` holds 2*n1 floats.
+// Returns the GuessStatus; out[] receives the guessed parameters (NaN when the
+// reference leaves them unset).
+template <int MODEL, int G>
+__device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *xs, const float *ys,
+                             bool y_finite, float *scratch, float *out) {
+    constexpr int P = Model<MODEL>::P;
+    constexpr bool paired = Model<MODEL>::paired;
+    const float qnan = __int_as_float(0x7fffffff);
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        out[k] = qnan;
+    if (!xc.guess_ok || !y_finite)
+        return kGuessInvalid;
+    const int m = xc.m, count = xc.count, n1 = xc.n1;
+    // Edge medians (initial_guess.hpp:142-150).
+    for (int t = int(g.lane); t < 2 * n1; t += G) {
+        const int side = t / n1, j = t % n1;
+        scratch[t] = j < count ? ys[side ? m - count + j : j] : __int_as_float(0x7f800000);
+    }
+    g.sync();
+    bitonic_sort(g, scratch, n1, 2);
+    const float left_level = sorted_median(scratch, count);
+    const float right_level = sorted_median(scratch + n1, count);
+    g.sync();
+    // Union of both sorted sides: reverse the right run to make one bitonic sequence.
+    for (int t = int(g.lane); t < n1 / 2; t += G) {
+        const float a = scratch[n1 + t], b = scratch[2 * n1 - 1 - t];
+        scratch[n1 + t] = b;
+        scratch[2 * n1 - 1 - t] = a;
+    }
+    g.sync();
+    bitonic_merge(g, scratch, 2 * n1);
+    const float baseline = sorted_median(scratch, 2 * count);
+    g.sync();
+    const float slope = paired ? rdiv(rsub(right_level, left_level), rsub(xc.right_x, xc.left_x)) : 0.0f;
+    const float level = paired ? left_level : baseline;
+    if (!isfinite(slope))
+        return kGuessInvalid;
+    const Signal<MODEL> s{xs, ys, level, slope, xc.left_x, m};
+    {
+        bool finite = true;
+        for (int j = int(g.lane); j < m; j += G)
+            finite = finite && isfinite(s.at(j));
+        if (!g.all(finite))
+            return kGuessInvalid;
+    }
+    // Noise scale: 1.4826 * median of absolute edge deviations (initial_guess.hpp:163-169).
+    for (int t = int(g.lane); t < 2 * n1; t += G) {
+        float v = __int_as_float(0x7f800000);
+        if (t < count)
+            v = fabsf(rsub(ys[t], left_level));
+        else if (t >= n1 && t - n1 < count)
+            v = fabsf(rsub(ys[m - count + (t - n1)], right_level));
+        scratch[t] = v;
+    }
+    g.sync();
+    // Pack the right deviations next to the left ones, then sort all 2*n1.
+    bitonic_sort(g, scratch, 2 * n1, 1);
+    const float noise = rmul(1.4826f, sorted_median(scratch, 2 * count));
+    g.sync();
+    if (!isfinite(noise))
+        return kGuessInvalid;
+    // Tallest smoothed local maximum (initial_guess.hpp:170-179).
+    float height = 0.0f;
+    int first = m;
+    for (int j = 1 + int(g.lane); j + 1 < m; j += G) {
+        const float v = s.smooth(j);
+        if (v > 0.0f && v > s.smooth(j - 1) && v >= s.smooth(j + 1) && v > height) {
+            height = v;
+            first = j;
+        }
+    }
+    argmax_pair(g, height, first);
+    if (first == m || height <= rmul(3.0f, noise))
+        return kGuessNoPeak;
+    first = s.raw_maximum(first);
+    PeakFeature primary = find_peak<MODEL, G>(g, s, xs, first, 0, m - 1, false);
+    if (!primary.valid)
+        return kGuessNoPeak;
+    if constexpr (!paired) {
+        out[0] = primary.amplitude;
+        out[1] = primary.center;
+        if constexpr (MODEL == kGaussian)
+            out[2] = rdiv(primary.width, 2.354820045030949382f);
+        else if constexpr (MODEL == kLorentzian)
+            out[2] = rdiv(primary.width, 2.0f);
+        else {
+            out[2] = primary.width;
+            out[3] = 0.5f;
+        }
+    } else {
+        // Second peak (initial_guess.hpp:199-227): the tallest smoothed local maximum
+        // that is far enough from the first and prominent enough.  Candidates are
+        // visited from tallest to shortest; only the prominence test is expensive.
+        const float separation =
+            smax(rmul(3.0f, xc.guess_spacing), rmul(2.0f, smin(primary.left_radius, primary.right_radius)));
+        const float threshold = rmul(3.0f, noise);
+        float bound_v = __int_as_float(0x7f800000);
+        int bound_j = -1;
+        int second = m;
+        while (true) {
+            float bv = 0.0f;
+            int bj = m;
+            for (int j = 1 + int(g.lane); j + 1 < m; j += G) {
+                const float v = s.smooth(j);
+                if (!(v > 0.0f && v > s.smooth(j - 1) && v >= s.smooth(j + 1)))
+                    continue;
+                if (!(v < bound_v || (v == bound_v && j > bound_j)))
+                    continue;
+                if (!(v > bv || (v == bv && j < bj)))
+                    continue;
+                const int idx = s.raw_maximum(j);
+                const int bins = idx > first ? idx - first : first - idx;
+                if (bins < 3 || fabsf(rsub(xs[idx], primary.center)) < separation)
+                    continue;
+                bv = v;
+                bj = j;
+            }
+            argmax_pair(g, bv, bj);
+            if (bj == m)
+                break;
+            if (prominence<MODEL, G>(g, s, bj) > threshold) {
+                second = s.raw_maximum(bj);
+                break;
+            }
+            bound_v = bv;
+            bound_j = bj;
+        }
+        if (second == m)
+            return kGuessInsufficient;
+        if (first > second) {
+            const int t = first;
+            first = second;
+            second = t;
+        }
+        // First minimum of signal[first+1 .. second-1].
+        float mv = __int_as_float(0x7f800000);
+        int mi = second;
+        for (int j = first + 1 + int(g.lane); j < second; j += G) {
+            const float v = s.at(j);
+            if (v < mv) {
+                mv = v;
+                mi = j;
+            }
+        }
+#pragma unroll
+        for (int o = G / 2; o >= 1; o >>= 1) {
+            const float ov = g.xor_(mv, o);
+            const int oi = g.xor_(mi, o);
+            if (ov < mv || (ov == mv && oi < mi)) {
+                mv = ov;
+                mi = oi;
+            }
+        }
+        const int valley = mi;
+        primary = find_peak<MODEL, G>(g, s, xs, first, 0, valley, true);
+        const PeakFeature secondary = find_peak<MODEL, G>(g, s, xs, second, valley, m - 1, true);
+        if (!primary.valid || !secondary.valid || !(primary.center < secondary.center))
+            return kGuessInsufficient;
+        out[0] = primary.amplitude;
+        out[1] = primary.center;
+        out[2] = rdiv(primary.width, 2.0f);
+        out[3] = secondary.amplitude;
+        out[4] = secondary.center;
+        out[5] = rdiv(secondary.width, 2.0f);
+        out[6] = rsub(left_level, rmul(slope, xc.left_x));
+        out[7] = slope;
+    }
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        if (!isfinite(out[k]))
+            return kGuessInvalid;
+    if (!(out[2] > 0.0f) || (paired && !(out[5] > 0.0f)))
+        return kGuessInvalid;
+    return kGuessSuccess;
+}
+
+} // namespace bf

@@ -1,0 +1,512 @@
+// Bounded Levenberg-Marquardt for one spectrum per thread group.
+//
+// Semantics follow cpu::fit_single (include/batchfit/cpu/solver.hpp:195-342) and
+// cpu::estimate_uncertainty (include/batchfit/cpu/uncertainty.hpp:12-110):
+// preflight, projection, degenerate-data diagnosis, active set, damped Cholesky,
+// gain-ratio damping update, the three stop rules and all six statuses.
+//
+// The B200 arrangement:
+//  * one fused pass per trial point evaluates chi2, J^T r and J^T J together
+//    (FP32 model/Jacobian, per-lane FP32 partial sums, two-sum reduce-scatter
+//    across the group, results as FP64 in shared memory).  A rejected trial
+//    leaves the accepted state untouched, so the reference's re-linearisation at
+//    an unchanged point is never recomputed;
+//  * every group lane runs the P x P control redundantly in FP64 (damped
+//    Cholesky, predicted reduction, gain ratio, lambda) -- no broadcasts needed;
+//  * the information matrix for the covariance is the accepted state's J^T J,
+//    inverted in FP64 (one factorisation, P triangular solves).
+#pragma once
+
+#include "bf_args.h"
+#include "bf_device.cuh"
+#include "bf_guess.cuh"
+#include "bf_models.cuh"
+
+namespace bf {
+
+enum FitStatus : int {
+    kConverged = 0,
+    kMaxIterations = 1,
+    kSingular = 2,
+    kInvalid = 3,
+    kDegenerate = 4,
+    kUnresolved = 5
+};
+enum UncertaintyStatus : int {
+    kAvailable = 0,
+    kNotConverged = 1,
+    kInsufficientDof = 2,
+    kUSingular = 3,
+    kActiveBound = 4,
+    kUInvalid = 5
+};
+
+constexpr double kFltEps = 1.1920928955078125e-07;
+constexpr double kDblEps = 2.220446049250313080847e-16;
+
+template <int MODEL> struct Layout {
+    static constexpr int P = Model<MODEL>::P;
+    static constexpr int K = 1 + P + P * (P + 1) / 2; // chi2, g[P], lower(A)
+    static constexpr int KP = pow2ceil(K);
+    __host__ __device__ static constexpr int tri(int k, int l) { return 1 + P + k * (k + 1) / 2 + l; }
+};
+
+// Points a lane accumulates naively before folding chi2 and J^T r into its
+// compensated running sums.
+constexpr int kChunk = 8;
+
+// One fused pass at parameters p: state[0] = chi2, state[1..P] = J^T r,
+// state[tri(k,l)] = (J^T J)_kl, as FP64 values.
+//
+// Accumulation: each lane sums kChunk points naively, then folds the chunk's chi2
+// and J^T r into Kahan pairs (numerics::add, numerics.hpp:12-18); the pairs enter
+// the group's two-sum tree with their low parts.  J^T r decides where the
+// iteration stops (its error moves the fixed point), so it gets the compensation;
+// J^T J only shapes the step and keeps plain per-lane sums.
+template <int MODEL, int G>
+__device__ __forceinline__ void lm_pass(const Group<G> &g, const float *xs, const float *ys, int m,
+                                        const float *p, double *state) {
+    using L = Layout<MODEL>;
+    constexpr int P = L::P;
+    const auto q = Model<MODEL>::prepare(p);
+    float hi[L::KP], lo[L::KP];
+#pragma unroll
+    for (int i = 0; i < L::KP; ++i) {
+        hi[i] = 0.0f;
+        lo[i] = 0.0f;
+    }
+    for (int base = int(g.lane); base < m; base += G * kChunk) {
+        float part[1 + P];
+#pragma unroll
+        for (int i = 0; i <= P; ++i)
+            part[i] = 0.0f;
+#pragma unroll
+        for (int c = 0; c < kChunk; ++c) {
+            const int j = base + c * G;
+            if (j < m) {
+                float J[P];
+                const float f = Model<MODEL>::eval(q, xs[j], J);
+                const float r = ys[j] - f;
+                part[0] = fmaf(r, r, part[0]);
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    part[1 + k] = fmaf(J[k], r, part[1 + k]);
+#pragma unroll
+                    for (int l = 0; l <= k; ++l)
+                        hi[L::tri(k, l)] = fmaf(J[k], J[l], hi[L::tri(k, l)]);
+                }
+            }
+        }
+        // Kahan fold; lo holds minus the Kahan correction, so the value is hi + lo.
+#pragma unroll
+        for (int i = 0; i <= P; ++i) {
+            const float adjusted = __fadd_rn(part[i], lo[i]);
+            const float next = __fadd_rn(hi[i], adjusted);
+            lo[i] = __fsub_rn(adjusted, __fsub_rn(next, hi[i]));
+            hi[i] = next;
+        }
+    }
+    reduce_scatter_store<G, L::KP>(g, hi, lo, state, L::K);
+    g.sync();
+}
+
+// In-place Cholesky of a packed lower triangle (FP64) and solve of rhs.
+// Mirrors detail::cholesky_solve (solver.hpp:98-143), including the optional
+// diagonal equilibration and every finiteness/positivity rejection.
+template <int P>
+__device__ __forceinline__ bool chol_solve(double (&a)[P * (P + 1) / 2], double (&b)[P], bool scaled) {
+    auto at = [](int i, int j) { return i * (i + 1) / 2 + j; };
+    double scale[P];
+    if (scaled) {
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+            const double d = a[at(i, i)];
+            if (!isfinite(d) || d <= 0.0)
+                return false;
+            scale[i] = sqrt(d);
+        }
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+            b[i] /= scale[i];
+#pragma unroll
+            for (int j = 0; j <= i; ++j)
+                a[at(i, j)] = (a[at(i, j)] / scale[i]) / scale[j];
+        }
+    }
+    double inv[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            double v = a[at(i, j)];
+#pragma unroll
+            for (int k = 0; k < j; ++k)
+                v -= a[at(i, k)] * a[at(j, k)];
+            if (!isfinite(v) || (i == j && v <= 0.0))
+                return false;
+            if (i == j) {
+                const double d = sqrt(v);
+                a[at(i, i)] = d;
+                inv[i] = 1.0 / d;
+            } else {
+                a[at(i, j)] = v * inv[j];
+            }
+        }
+        double v = b[i];
+#pragma unroll
+        for (int j = 0; j < i; ++j)
+            v -= a[at(i, j)] * b[j];
+        b[i] = v * inv[i];
+    }
+#pragma unroll
+    for (int i = P - 1; i >= 0; --i) {
+        double v = b[i];
+#pragma unroll
+        for (int j = i + 1; j < P; ++j)
+            v -= a[at(j, i)] * b[j];
+        b[i] = v * inv[i];
+        if (!isfinite(b[i]))
+            return false;
+    }
+    if (scaled) {
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+            b[i] /= scale[i];
+            if (!isfinite(b[i]))
+                return false;
+        }
+    }
+    return true;
+}
+
+// free_shape (solver.hpp:70-82).
+template <int MODEL> __device__ __forceinline__ bool free_shape(const FitArgs &a) {
+    bool free = a.lower[1] != a.upper[1] || a.lower[2] != a.upper[2];
+    if constexpr (MODEL == kPseudoVoigt)
+        free = free || a.lower[3] != a.upper[3];
+    if constexpr (MODEL == kTwoLorentzian)
+        free = free || a.lower[4] != a.upper[4] || a.lower[5] != a.upper[5];
+    return free;
+}
+
+// spectral_success (solver.hpp:83-96).
+template <int MODEL> __device__ __forceinline__ int spectral_success(const float *p, float spacing) {
+    constexpr float factor = Model<MODEL>::width_factor;
+    if (spacing > 0.0f && fabsf(p[2]) * factor < spacing)
+        return kUnresolved;
+    if constexpr (MODEL == kTwoLorentzian)
+        if (spacing > 0.0f && fabsf(p[5]) * factor < spacing)
+            return kUnresolved;
+    return kConverged;
+}
+
+struct FitOutcome {
+    int status;
+    uint32_t iterations;
+    double chi2;
+};
+
+// The LM iteration proper (fit_single after the input copy).  `p` enters as the
+// initial values and leaves as the reported parameters.  `state` holds two
+// K-slot FP64 state blocks in shared memory.
+template <int MODEL, int G>
+__device__ FitOutcome lm_solve(const Group<G> &g, const FitArgs &a, const XConst &xc, const float *xs,
+                               const float *ys, bool y_finite, bool y_flat, double syy, float (&p)[Model<MODEL>::P],
+                               double *state, int &cur_slot) {
+    using L = Layout<MODEL>;
+    constexpr int P = L::P;
+    FitOutcome out{kInvalid, 0u, __longlong_as_double(0x7ff8000000000000ll)};
+    const int m = xc.m;
+    bool init_finite = true;
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        init_finite = init_finite && isfinite(p[k]);
+    if (!a.options_ok || !init_finite || !xc.x_finite || !y_finite)
+        return out;
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        p[k] = sclamp(p[k], a.lower[k], a.upper[k]);
+    double *cur = state + cur_slot * L::K;
+    lm_pass<MODEL, G>(g, xs, ys, m, p, cur);
+    double chi2 = cur[0];
+    if (!isfinite(chi2))
+        return out;
+    out.chi2 = chi2;
+    if (xc.varied_x && y_flat && free_shape<MODEL>(a)) {
+        out.status = kDegenerate;
+        return out;
+    }
+    const bool parity = a.policy == kPolicyParity;
+    const double eps_t = parity ? kDblEps : kFltEps;
+    double lambda = a.lambda0;
+    const double lambda_max = fmax(a.lambda0, 1.0 / kFltEps);
+    out.status = kMaxIterations;
+    const double floor_g = a.noise_floor * kFltEps * sqrt(syy);
+    for (uint32_t it = 0; it < a.max_iterations; ++it) {
+        // Accepted-state finiteness (the reference's linearize() check).  A and g
+        // stay in shared memory; lanes read them as broadcasts when needed.
+        const double *A = cur + 1 + P; // packed lower triangle
+        const double *gr = cur + 1;
+        bool finite = true;
+#pragma unroll
+        for (int i = 0; i < L::K - 1; ++i)
+            finite = finite && isfinite(cur[1 + i]);
+        if (!finite) {
+            out.status = kInvalid;
+            break;
+        }
+        bool active[P];
+        double gnorm = 0.0;
+        bool at_floor = true;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const double gk = gr[k];
+            active[k] = a.lower[k] == a.upper[k] || (p[k] == a.lower[k] && gk < 0.0) ||
+                        (p[k] == a.upper[k] && gk > 0.0);
+            if (!active[k]) {
+                gnorm = fmax(gnorm, fabs(gk));
+                at_floor = at_floor && fabs(gk) <= floor_g * sqrt(fmax(A[k * (k + 1) / 2 + k], 0.0));
+            }
+        }
+        if (gnorm <= a.gtol || (parity && at_floor)) {
+            out.status = spectral_success<MODEL>(p, xc.spacing);
+            break;
+        }
+        double D[P * (P + 1) / 2], delta[P];
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            delta[k] = active[k] ? 0.0 : gr[k];
+#pragma unroll
+            for (int l = 0; l <= k; ++l) {
+                double v = A[k * (k + 1) / 2 + l];
+                if (active[k] || active[l])
+                    v = 0.0;
+                if (k == l)
+                    v = active[k] ? 1.0 : v + lambda * A[k * (k + 1) / 2 + k];
+                D[k * (k + 1) / 2 + l] = v;
+            }
+        }
+        out.iterations = it + 1;
+        if (!chol_solve<P>(D, delta, (a.flags & kFlagScaledCholesky) != 0u)) {
+            out.status = kSingular;
+            break;
+        }
+        float trial[P];
+        double step_norm = 0.0, param_norm = 0.0;
+        bool finite_trial = true;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            step_norm = fmax(step_norm, fabs(delta[k]));
+            trial[k] = float(dclamp(double(p[k]) + delta[k], double(a.lower[k]), double(a.upper[k])));
+            finite_trial = finite_trial && isfinite(trial[k]);
+            delta[k] = double(trial[k]) - double(p[k]);
+            param_norm = fmax(param_norm, fabs(double(p[k])));
+        }
+        const double damp = fmax(1.0, lambda);
+        if (step_norm <= a.xtol * (param_norm + a.xtol) / damp ||
+            (parity && step_norm * damp <= a.step_quantum * kFltEps * param_norm)) {
+            out.status = spectral_success<MODEL>(p, xc.spacing);
+            break;
+        }
+        double predicted = 0.0;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            predicted += 2.0 * gr[k] * delta[k];
+#pragma unroll
+            for (int l = 0; l < P; ++l) {
+                const double akl = k >= l ? A[k * (k + 1) / 2 + l] : A[l * (l + 1) / 2 + k];
+                predicted -= delta[k] * akl * delta[l];
+            }
+        }
+        double trial_cost = __longlong_as_double(0x7ff8000000000000ll);
+        double *nxt = state + (1 - cur_slot) * L::K;
+        if (finite_trial) {
+            lm_pass<MODEL, G>(g, xs, ys, m, trial, nxt);
+            trial_cost = nxt[0];
+        }
+        const double reduction = chi2 - trial_cost;
+        const double threshold = a.ftol * chi2;
+        const bool small = isfinite(trial_cost) && isfinite(predicted) && predicted >= 0.0 &&
+                           fabs(reduction) <= threshold && predicted <= threshold / damp;
+        if (isfinite(trial_cost) && reduction > 0.0 && isfinite(predicted) && predicted > 0.0) {
+#pragma unroll
+            for (int k = 0; k < P; ++k)
+                p[k] = trial[k];
+            chi2 = trial_cost;
+            cur_slot = 1 - cur_slot;
+            cur = nxt;
+            const double ratio = reduction / predicted;
+            const double u = 2.0 * ratio - 1.0;
+            const double factor = ratio >= 1.0 ? 1.0 / 3.0 : fmax(1.0 / 3.0, 1.0 - u * u * u);
+            lambda = dclamp(lambda * factor, eps_t, lambda_max);
+        } else {
+            lambda = fmin(lambda_max, lambda * 10.0);
+        }
+        // Every lane must finish reading `nxt` before a later pass overwrites it.
+        g.sync();
+        if (small) {
+            out.status = spectral_success<MODEL>(p, xc.spacing);
+            break;
+        }
+    }
+    out.chi2 = chi2;
+    return out;
+}
+
+// Covariance from the accepted state's information matrix, FP64 inverse
+// (uncertainty.hpp:12-110), written to cov_out[P*P], se_out[P] (global memory).
+// `state` is the group's two-slot block; `cur` points at the accepted slot.  The
+// inverse columns are staged in `state` (both slots) once H sits in registers.
+template <int MODEL, int G>
+__device__ int lm_uncertainty(const Group<G> &g, const FitArgs &a, const XConst &xc,
+                              const float (&p)[Model<MODEL>::P], int fit_status, float chi2f, double *state,
+                              const double *cur, bool parity, float *cov_out, float *se_out) {
+    using L = Layout<MODEL>;
+    constexpr int P = L::P;
+    constexpr int T = P * (P + 1) / 2;
+    int status = kAvailable;
+    bool fixed[P];
+    int nfree = 0;
+    double H[T];
+    double scale[P], inv[P];
+    double variance = 0.0;
+    if (fit_status != kConverged)
+        status = kNotConverged;
+    else if (!isfinite(chi2f) || chi2f < 0.0f)
+        status = kUInvalid;
+    if (status == kAvailable) {
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            if (status != kAvailable)
+                break;
+            if (!isfinite(p[k]) || isnan(a.lower[k]) || isnan(a.upper[k]) || a.lower[k] > a.upper[k] ||
+                p[k] < a.lower[k] || p[k] > a.upper[k]) {
+                status = kUInvalid;
+                break;
+            }
+            fixed[k] = a.lower[k] == a.upper[k];
+            nfree += fixed[k] ? 0 : 1;
+            if (!fixed[k] && (p[k] == a.lower[k] || p[k] == a.upper[k]))
+                status = kActiveBound;
+        }
+    }
+    if (status == kAvailable && xc.m <= nfree)
+        status = kInsufficientDof;
+    if (status == kAvailable && !xc.x_finite)
+        status = kUInvalid;
+    if (status == kAvailable) {
+#pragma unroll
+        for (int k = 0; k < P; ++k)
+#pragma unroll
+            for (int l = 0; l <= k; ++l) {
+                double v = cur[L::tri(k, l)];
+                if (!isfinite(v))
+                    status = kUInvalid;
+                if (fixed[k] || fixed[l])
+                    v = (k == l) ? 1.0 : 0.0;
+                H[k * (k + 1) / 2 + l] = v;
+            }
+        variance = double(chi2f) / double(xc.m - nfree);
+        if (!isfinite(variance))
+            status = kUInvalid;
+    }
+    if (status == kAvailable) {
+        // One equilibrated factorisation; the reference refactors per column with
+        // the same deterministic result.
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+            const double d = H[i * (i + 1) / 2 + i];
+            if (!isfinite(d) || d <= 0.0)
+                status = kUSingular;
+            scale[i] = sqrt(d);
+        }
+        if (status == kAvailable) {
+#pragma unroll
+            for (int i = 0; i < P; ++i)
+#pragma unroll
+                for (int j = 0; j <= i; ++j)
+                    H[i * (i + 1) / 2 + j] = (H[i * (i + 1) / 2 + j] / scale[i]) / scale[j];
+            const double pivot_floor = 64.0 * (parity ? kDblEps : kFltEps);
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+#pragma unroll
+                for (int j = 0; j <= i; ++j) {
+                    double v = H[i * (i + 1) / 2 + j];
+#pragma unroll
+                    for (int k = 0; k < j; ++k)
+                        v -= H[i * (i + 1) / 2 + k] * H[j * (j + 1) / 2 + k];
+                    if (!isfinite(v) || (i == j && v <= 0.0))
+                        status = kUSingular;
+                    if (i == j) {
+                        const double d = sqrt(v);
+                        H[i * (i + 1) / 2 + i] = d;
+                        inv[i] = 1.0 / d;
+                    } else {
+                        H[i * (i + 1) / 2 + j] = v * inv[j];
+                    }
+                }
+            }
+            if (status == kAvailable) {
+#pragma unroll
+                for (int i = 0; i < P; ++i)
+                    if (!fixed[i] && H[i * (i + 1) / 2 + i] * H[i * (i + 1) / 2 + i] <= pivot_floor)
+                        status = kUSingular;
+            }
+        }
+    }
+    g.sync(); // every lane has read `cur`; the state block becomes column storage
+    if (status == kAvailable) {
+#pragma unroll
+        for (int column = 0; column < P; ++column) {
+            double b[P];
+#pragma unroll
+            for (int i = 0; i < P; ++i)
+                b[i] = (i == column) ? 1.0 / scale[i] : 0.0;
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                double v = b[i];
+#pragma unroll
+                for (int j = 0; j < i; ++j)
+                    v -= H[i * (i + 1) / 2 + j] * b[j];
+                b[i] = v * inv[i];
+            }
+#pragma unroll
+            for (int i = P - 1; i >= 0; --i) {
+                double v = b[i];
+#pragma unroll
+                for (int j = i + 1; j < P; ++j)
+                    v -= H[j * (j + 1) / 2 + i] * b[j];
+                b[i] = v * inv[i];
+            }
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                const double c = fixed[column] || fixed[i] ? 0.0 : (b[i] / scale[i]) * variance;
+                if (!isfinite(c))
+                    status = kUInvalid;
+                if (int(g.lane) == (i * P + column) % G)
+                    state[i * P + column] = c;
+            }
+        }
+    }
+    g.sync();
+    bool negative = false;
+    if (status == kAvailable) {
+#pragma unroll
+        for (int i = 0; i < P; ++i)
+            negative = negative || state[i * P + i] < 0.0;
+        if (negative)
+            status = kUInvalid;
+    }
+    const float qnan = __int_as_float(0x7fffffff);
+    for (int k = int(g.lane); k < P * P; k += G) {
+        const int i = k / P, j = k % P;
+        const float v = status == kAvailable ? float(state[i * P + j] / 2.0 + state[j * P + i] / 2.0) : qnan;
+        cov_out[k] = i == j && status == kAvailable ? float(state[k]) : v;
+    }
+    for (int k = int(g.lane); k < P; k += G)
+        se_out[k] = status == kAvailable ? float(sqrt(state[k * P + k])) : qnan;
+    g.sync();
+    return status;
+}
+
+} // namespace bf

@@ -1,0 +1,157 @@
+/* batchfit_cuda.h -- C ABI of the batchfit B200 (sm_100a) fitting backend.
+ *
+ * A drop-in CUDA device for batchfit's fit path: shared x[M], fit-major y[N,M],
+ * optional initial values p0[N,P] (NULL -> data-only guesses on the GPU), common
+ * lower/upper bounds (equal bounds fix a coordinate), outputs params[N,P],
+ * status/iterations/chi2[N] and optional covariance[N,P,P], stderr[N,P],
+ * uncertainty_status[N].  Plain pointers and sizes only; no CUDA or framework types.
+ *
+ * Reference interfaces each entry point replaces (paths inside the batchfit project):
+ *   bf_cuda_context_create/destroy  metal::Context (include/batchfit/metal/batch.hpp:160-174)
+ *   bf_cuda_fit                     fit_batch<Model>(SharedBatch&, Device, options)
+ *                                   (include/batchfit/metal/batch.hpp:268-310) and the Python
+ *                                   native entry _core.fit (python/bindings.cpp:200-207)
+ *   bf_cuda_submit / _ready / _wait submit_batch<Model> -> PendingBatch{ready(),get()}
+ *                                   (include/batchfit/metal/batch.hpp:198-217,253-264)
+ *   bf_cuda_guess                   cpu::initial_guess<float,Model> per row
+ *                                   (include/batchfit/cpu/initial_guess.hpp:120-249)
+ *   bf_solver_options               cpu::SolverOptions<float,P> (include/batchfit/cpu/solver.hpp:26-41)
+ *   status / uncertainty codes      FitStatus (solver.hpp:16-23), UncertaintyStatus
+ *                                   (include/batchfit/uncertainty_types.hpp:3-10)
+ *   bf_cuda_available               batchfit.metal_available() (python/batchfit/__init__.py:51-53)
+ *
+ * Ownership: the caller owns every input and output buffer; the library owns its
+ * device staging buffers, streams and events.  Threading: calls on one context are
+ * serialised internally.  Per-fit failures are status codes, never error returns;
+ * argument, device and CUDA failures return a nonzero code with a message from
+ * bf_cuda_last_error() (thread-local).
+ */
+#ifndef BATCHFIT_CUDA_H
+#define BATCHFIT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes. */
+#define BF_OK 0
+#define BF_ERR_INVALID_ARGUMENT 1 /* std::invalid_argument in the reference */
+#define BF_ERR_CUDA 2             /* a CUDA runtime error (std::runtime_error) */
+#define BF_ERR_UNAVAILABLE 3      /* no usable sm_100 device */
+#define BF_ERR_BUSY 4             /* a pending submission still owns the context */
+
+/* Model ids (python/batchfit/__init__.py:13). */
+#define BF_MODEL_GAUSSIAN 0       /* amplitude, center, sigma */
+#define BF_MODEL_LORENTZIAN 1     /* amplitude, center, hwhm */
+#define BF_MODEL_PSEUDO_VOIGT 2   /* amplitude, center, fwhm, mixing */
+#define BF_MODEL_TWO_LORENTZIAN 3 /* a1, c1, hwhm1, a2, c2, hwhm2, intercept, slope */
+
+/* Where the pointers of one call live. */
+#define BF_MEMORY_HOST 0   /* host memory (pinned memory overlaps copies with compute) */
+#define BF_MEMORY_DEVICE 1 /* device memory of the context's GPU */
+
+/* Stopping policy.
+ * BF_POLICY_REFERENCE: the reference float solver's stop rules with the given
+ *   tolerances (defaults 1e-5 / 1e-6 / 1e-6).
+ * BF_POLICY_PARITY: stop rules aimed at the float64 solution: the double-precision
+ *   tolerances (1e-10 / 1e-10 / 1e-12) plus two float32 noise-floor tests -- every
+ *   free |g_k| <= noise_floor * FLT_EPSILON * sqrt(A_kk * sum(y^2)), or an undamped
+ *   step <= step_quantum * FLT_EPSILON * max|p|.  Statuses keep their meaning. */
+#define BF_POLICY_REFERENCE 0
+#define BF_POLICY_PARITY 1
+
+typedef struct bf_solver_options {
+    uint32_t max_iterations;   /* 100 */
+    double initial_lambda;     /* 1e-3 */
+    double gradient_tolerance; /* see BF_POLICY_* */
+    double step_tolerance;
+    double cost_tolerance;
+    uint32_t compensated_sum; /* accepted for API parity: sums are always compensated */
+    uint32_t scaled_cholesky; /* diagonal equilibration in the damped solve */
+    uint32_t policy;          /* BF_POLICY_* */
+    double noise_floor;       /* parity policy, multiples of FLT_EPSILON (16) */
+    double step_quantum;      /* parity policy, multiples of FLT_EPSILON (16) */
+    float lower[8];           /* per-parameter bounds, first P used; -inf/inf = unbounded */
+    float upper[8];
+} bf_solver_options;
+
+typedef struct bf_fit_args {
+    int32_t model;     /* BF_MODEL_* */
+    uint64_t n;        /* fits */
+    uint32_t m;        /* points per fit */
+    const float *x;    /* [M] shared grid */
+    const float *y;    /* [N*M] fit-major observations */
+    const float *p0;   /* [N*P] initial values, or NULL for data-only guesses */
+    int32_t memory;    /* BF_MEMORY_* for x, y, p0 and every output */
+    int32_t uncertainties;
+    int32_t group_lanes; /* 0 = tuned choice, else 8, 16 or 32 lanes per fit */
+    bf_solver_options options;
+} bf_fit_args;
+
+typedef struct bf_fit_outputs {
+    float *params;              /* [N*P] */
+    int32_t *status;            /* [N] FitStatus */
+    uint32_t *iterations;       /* [N] */
+    float *chi2;                /* [N] unweighted sum of squared residuals */
+    float *covariance;          /* [N*P*P] when uncertainties */
+    float *standard_errors;     /* [N*P] when uncertainties */
+    int32_t *uncertainty_status;/* [N] when uncertainties */
+} bf_fit_outputs;
+
+typedef struct bf_cuda_context bf_cuda_context;
+typedef struct bf_cuda_pending bf_cuda_pending;
+
+/* Timing of the last completed call on a context (CUDA events, milliseconds). */
+typedef struct bf_cuda_timing {
+    double kernel_ms;   /* fit kernel(s) only */
+    double total_ms;    /* whole call including copies */
+    uint32_t launches;  /* fit kernel launches */
+    int32_t group_lanes;
+    int32_t grid;
+    int32_t blocks_per_sm;
+} bf_cuda_timing;
+
+const char *bf_cuda_last_error(void);
+/* 1 when an sm_100-class device is present and usable. */
+int bf_cuda_available(void);
+int bf_cuda_version(void); /* library version, 100 * major + minor */
+
+int bf_cuda_context_create(int device, bf_cuda_context **out);
+void bf_cuda_context_destroy(bf_cuda_context *ctx);
+
+/* Reference defaults for `model` under `policy`, bounds set to -inf/+inf. */
+int bf_cuda_default_options(int32_t model, uint32_t policy, bf_solver_options *out);
+
+/* Synchronous fit (submit + wait). */
+int bf_cuda_fit(bf_cuda_context *ctx, const bf_fit_args *args, const bf_fit_outputs *out);
+
+/* Asynchronous fit: the call returns once the work is queued on the GPU.  The
+ * input and output buffers must stay valid and untouched until bf_cuda_wait. */
+int bf_cuda_submit(bf_cuda_context *ctx, const bf_fit_args *args, const bf_fit_outputs *out,
+                   bf_cuda_pending **pending);
+/* 1 when the submission has completed, 0 when still running, <0 on error. */
+int bf_cuda_ready(bf_cuda_pending *pending);
+/* Waits, releases `pending` and returns the submission's result code. */
+int bf_cuda_wait(bf_cuda_pending *pending);
+
+/* Data-only guesses only (initial_guess<float,Model> per row); params[N*P] and
+ * guess_status[N] (0 success, 1 invalid_input, 2 no_peak, 3 insufficient_peaks). */
+int bf_cuda_guess(bf_cuda_context *ctx, int32_t model, uint64_t n, uint32_t m, const float *x,
+                  const float *y, int32_t memory, float *params, int32_t *guess_status);
+
+int bf_cuda_last_timing(bf_cuda_context *ctx, bf_cuda_timing *out);
+
+/* Pinned host memory for BF_MEMORY_HOST calls that should overlap copies. */
+int bf_cuda_host_alloc(size_t bytes, void **out);
+int bf_cuda_host_free(void *ptr);
+
+/* Largest M the kernels support for `model` (shared-memory layout bound). */
+uint32_t bf_cuda_max_points(int32_t model);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,313 @@
+"""GPU LM fits through the C ABI, checked against the CPU oracle.
+
+* policy="reference": the reference float solver's stop rules, compared with the
+  oracle's float path at the reference's own GPU parity bar
+  (tests/metal_lm_checks.hpp:41-45: params atol=rtol=2e-4, chi2 atol 1e-6 /
+  rtol 2e-5, exact status).
+* policy="parity" (default): compared with the float64 oracle at 1e-4 relative
+  parameter error (unit floors: centers by the x span, mixing by 1), 1e-5 chi2
+  relative error and >= 99.9% status agreement.
+"""
+
+import numpy as np
+import pytest
+
+from batchfit_b200 import accuracy as A
+from batchfit_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+PARAM_TOL, CHI2_TOL, STATUS_AGREE = 1e-4, 1e-5, 0.999
+
+
+def synthetic(model, n, m, seed):
+    """Seeded spectra like the reference's CPU benchmark workload (SNR 20)."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(-10, 10, m)
+    a = rng.uniform(1, 3, n)
+    c = rng.uniform(-3, 3, n)
+    w = rng.uniform(0.6, 1.0, n) if model != "pseudo_voigt" else rng.uniform(1.4, 2.0, n)
+    if model == "gaussian":
+        clean = a[:, None] * np.exp(-0.5 * ((x - c[:, None]) / w[:, None]) ** 2)
+    elif model == "lorentzian":
+        clean = a[:, None] / (1 + ((x - c[:, None]) / w[:, None]) ** 2)
+    elif model == "pseudo_voigt":
+        eta = rng.uniform(0.2, 0.8, n)
+        z = (x - c[:, None]) / w[:, None]
+        clean = a[:, None] * ((1 - eta[:, None]) * np.exp(-4 * np.log(2) * z * z) + eta[:, None] / (1 + 4 * z * z))
+    else:
+        c1, c2 = rng.uniform(-6, -2, n), rng.uniform(2, 6, n)
+        w1, w2 = rng.uniform(0.5, 0.8, n), rng.uniform(0.5, 0.8, n)
+        clean = (a[:, None] / (1 + ((x - c1[:, None]) / w1[:, None]) ** 2)
+                 + 0.8 * a[:, None] / (1 + ((x - c2[:, None]) / w2[:, None]) ** 2)
+                 + rng.uniform(0.3, 0.5, n)[:, None] + rng.uniform(-0.02, 0.02, n)[:, None] * x)
+    sigma = np.sqrt(np.mean(clean ** 2, axis=1)) / 20
+    y = clean + sigma[:, None] * rng.normal(size=clean.shape)
+    x = x.astype(np.float32)
+    p = {"gaussian": 3, "lorentzian": 3, "pseudo_voigt": 4, "two_lorentzian": 8}[model]
+    lower = np.full(p, -np.inf, np.float32)
+    upper = np.full(p, np.inf, np.float32)
+    lower[0], lower[1], upper[1] = 0, x[0], x[-1]
+    lower[2], upper[2] = (x[1] - x[0]) / 8, x[-1] - x[0]
+    if p == 4:
+        lower[3], upper[3] = 0, 1
+    if p == 8:
+        lower[3], lower[4], upper[4] = 0, x[0], x[-1]
+        lower[5], upper[5] = lower[2], upper[2]
+    return x, y.astype(np.float32), lower, upper
+
+
+def fallback_p0(oracle, model, x, y):
+    """Guesses with the reference benchmark's fallback rows (bench/cpu_workload.hpp:126-141)."""
+    p0, status, _ = oracle.guess("port", model, x, y, np.float32)
+    fallback = {3: [2, 0, 0.8], 4: [2, 0, 1.7, 0.5], 8: [2, -1.5, 0.65, 2, 1.5, 0.65, 0.4, 0]}[p0.shape[1]]
+    p0[status != 0] = fallback
+    return p0
+
+
+@pytest.mark.parametrize("model", ["gaussian", "lorentzian", "pseudo_voigt", "two_lorentzian"])
+@pytest.mark.parametrize("n", [1, 31, 32, 33, 257])
+@pytest.mark.parametrize("m", [32, 129])
+def test_reference_policy_matches_oracle_float(bf, oracle, model, n, m):
+    x, y, lo, hi = synthetic(model, n, m, seed=20261107 + n + m)
+    p0 = fallback_p0(oracle, model, x, y)
+    got = bf.fit(x, y, model, p0, (lo, hi), "cuda", policy="reference")
+    ref = oracle.fit("port", model, x, y, p0, lo, hi, np.float32)
+    np.testing.assert_array_equal(got.status, ref.status)
+    ok = ref.status == 0
+    np.testing.assert_allclose(got.params[ok], ref.params[ok], atol=2e-4, rtol=2e-4)
+    np.testing.assert_allclose(got.chi2[ok], ref.chi2[ok], atol=1e-6, rtol=2e-5)
+    assert np.all(got.iterations <= 100)
+
+
+@pytest.mark.parametrize("model", ["gaussian", "lorentzian", "pseudo_voigt", "two_lorentzian"])
+def test_parity_policy_matches_oracle_double(bf, oracle, model):
+    x, y, lo, hi = synthetic(model, 2000, 257, seed=7 + len(model))
+    got = bf.fit(x, y, model, None, (lo, hi), "cuda")
+    ref = oracle.fit("port", model, x, y, None, lo, hi, np.float64)
+    s = A.summarize(model, x, y, got.params, got.status, got.chi2, ref.params, ref.status, ref.chi2,
+                    PARAM_TOL, CHI2_TOL)
+    assert s["status_agreement"] >= STATUS_AGREE, s
+    assert s["within_tol_fraction"] >= STATUS_AGREE, s
+
+
+def test_lorentzian_small_parity(bf, oracle):
+    w = W.lorentzian_small()
+    got = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda", uncertainties=True)
+    ref = oracle.fit("port", w.model, w.x, w.y, None, w.lower, w.upper, np.float64, uncertainties=True)
+    assert np.all(got.status == 0) and np.all(ref.status == 0)
+    s = A.summarize(w.model, w.x, w.y, got.params, got.status, got.chi2, ref.params, ref.status, ref.chi2,
+                    PARAM_TOL, CHI2_TOL)
+    assert s["within_tol_fraction"] == 1.0, s
+    np.testing.assert_array_equal(got.uncertainty_status, ref.uncertainty_status)
+    ok = got.uncertainty_status == 0
+    np.testing.assert_allclose(got.stderr[ok], ref.stderr[ok], rtol=1e-3)
+    np.testing.assert_allclose(got.covariance[ok], ref.covariance[ok], rtol=2e-3, atol=1e-9)
+
+
+def test_pseudo_voigt_plain_sample_parity(bf, oracle):
+    w = W.pseudo_voigt_plain(n=20000)
+    got = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda", uncertainties=True)
+    ref = oracle.fit("port", w.model, w.x, w.y, None, w.lower, w.upper, np.float64, uncertainties=True)
+    s = A.summarize(w.model, w.x, w.y, got.params, got.status, got.chi2, ref.params, ref.status, ref.chi2,
+                    PARAM_TOL, CHI2_TOL)
+    assert s["status_agreement"] >= STATUS_AGREE, s
+    assert s["within_tol_fraction"] >= STATUS_AGREE, s
+    assert s["chi2_within_fraction"] >= STATUS_AGREE, s
+    agree = got.uncertainty_status == ref.uncertainty_status
+    assert agree.mean() >= STATUS_AGREE
+    ok = agree & (ref.uncertainty_status == 0)
+    rel = np.abs(got.stderr[ok] - ref.stderr[ok]) / np.abs(ref.stderr[ok])
+    assert np.quantile(rel, 0.999) <= 1e-2, np.quantile(rel, [0.5, 0.99, 0.999, 1.0])
+
+
+def test_row_failure_isolation(bf):
+    # python/tests/test_api.py:79-87
+    x = np.linspace(-4, 4, 129).astype(np.float32)
+    y = np.tile(2 / (1 + ((x - 0.2) / 0.7) ** 2), (5, 1)).astype(np.float32)
+    y[1, 10] = np.nan
+    y[2, 10] = np.inf
+    y[3] = 0
+    p0 = np.tile(np.array([1.8, 0, 0.8], np.float32), (5, 1))
+    for policy in ("reference", "parity"):
+        r = bf.fit(x, y, p0=p0, device="cuda", policy=policy)
+        np.testing.assert_array_equal(r.status, [0, 3, 3, 4, 0])
+        assert np.isnan(r.chi2[1]) and np.isnan(r.chi2[2])
+        np.testing.assert_array_equal(r.params[1], p0[1])
+    c = bf.fit(x, y[[0]], p0=p0[0], bounds=([0, 0.2, 0.7], [np.inf, 0.2, 0.7]), device="cuda")
+    np.testing.assert_allclose(c.params[0], [2, 0.2, 0.7], atol=2e-6)
+
+
+def test_failure_statuses(bf):
+    # tests/metal_lm_checks.hpp:86-155 on a degenerate 3-point grid
+    x = np.zeros(3, np.float32)
+    y = np.full((3, 3), 2, np.float32)
+    p0 = np.array([[1, 0, 1], [2, 0, 1], [1, 0, 0]], np.float32)
+    r = bf.fit(x, y, p0=p0, device="cuda", policy="reference")
+    np.testing.assert_array_equal(r.status, [2, 0, 3])
+    np.testing.assert_array_equal(r.iterations, [1, 0, 0])
+    o = bf.solver_options("lorentzian", [-np.inf] * 3, [np.inf] * 3, "reference", max_iterations=0)
+    z = bf.fit(x, y, p0=p0, device="cuda", options=o)
+    assert z.status[0] == 1 and z.chi2[0] == 3
+    o = bf.solver_options("lorentzian", [-np.inf, 0, 1], [np.inf, 0, 1], "reference")
+    f = bf.fit(x, y, p0=p0, device="cuda", options=o)
+    assert f.status[0] == 0 and f.params[0, 1] == 0 and f.params[0, 2] == 1
+    o = bf.solver_options("lorentzian", [-np.inf, 0, 1], [1.5, 0, 1], "reference")
+    cl = bf.fit(x, y, p0=p0, device="cuda", options=o)
+    assert np.all(cl.status == 0) and np.all(cl.params[:, 0] == 1.5)
+    o = bf.solver_options("lorentzian", [-np.inf] * 3, [np.inf] * 3, "reference", initial_lambda=0.0)
+    bad = bf.fit(x, y, p0=p0, device="cuda", options=o)
+    assert np.all(bad.status == 3)
+    xb = x.copy()
+    xb[0] = np.nan
+    inv = bf.fit(xb, y, p0=p0, device="cuda")
+    assert np.all(inv.status == 3)
+
+
+@pytest.mark.parametrize("model", ["gaussian", "lorentzian", "pseudo_voigt", "two_lorentzian"])
+def test_numerics_pathologies(bf, oracle, model):
+    # tests/numerics_checks.hpp:120-190
+    base = {3: [2, 0, 0.2], 4: [2, 0, 0.2, 0.4], 8: [2, -0.4, 0.12, 1.5, 0.4, 0.15, 0.2, 0.01]}
+    p = {"gaussian": 3, "lorentzian": 3, "pseudo_voigt": 4, "two_lorentzian": 8}[model]
+    x = (-1 + np.arange(129) / 64).astype(np.float32)
+    rows, inits = [], []
+    for i in range(9):
+        init = np.array(base[p], np.float32)
+        if i == 5:
+            init[1] = -1
+        if i == 6:
+            init[2] = 1e-4
+            if p == 8:
+                init[5] = 1e-4
+        if i == 8:
+            init[0] *= 1e30
+            if p == 8:
+                init[3] *= 1e30
+        inits.append(init)
+        rows.append(np.zeros(129) if i == 0 else np.full(129, 3.0) if i == 1
+                    else oracle.eval_model(model, x, init, np.float32))
+    y = np.array(rows, np.float32)
+    y[2, 17], y[3, 17], y[4, 17] = np.nan, np.inf, -np.inf
+    p0 = np.array(inits, np.float32)
+    for policy in ("reference", "parity"):
+        r = bf.fit(x, y, model, p0, device="cuda", policy=policy)
+        assert r.status[0] == 4 and r.status[1] == 4
+        assert np.all(r.status[2:5] == 3) and np.all(np.isnan(r.chi2[2:5]))
+        assert r.status[5] == 0 and r.status[6] == 5 and r.status[7] == 0
+        assert r.status[8] == 3
+        for i in (0, 1, 5, 6, 7):
+            assert np.isfinite(r.chi2[i]) and np.all(np.isfinite(r.params[i]))
+    xb = x.copy()
+    xb[17] = np.nan
+    r = bf.fit(xb, y, model, p0, device="cuda")
+    assert np.all(r.status == 3)
+
+
+def test_uncertainty_statuses(bf):
+    # python/tests/test_uncertainty.py:67-98
+    x = np.linspace(-5, 5, 129)
+    y = 2 / (1 + ((x - 0.2) / 0.7) ** 2)
+    failed = y.copy()
+    failed[17] = np.nan
+    r = bf.fit(x, failed, p0=[2, 0.2, 0.7], device="cuda", uncertainties=True)
+    assert r.status[0] == 3 and r.uncertainty_status[0] == 1
+    assert np.all(np.isnan(r.covariance)) and np.all(np.isnan(r.stderr))
+    sx = np.array([-1.0, 0.0, 1.0])
+    small = bf.fit(sx, 2 / (1 + (sx / 2) ** 2), p0=[2, 0, 2], device="cuda", uncertainties=True)
+    assert small.uncertainty_status[0] == 2
+    singular = bf.fit(np.zeros(20), np.full(20, 2.0), p0=[2, 0, 1], device="cuda", uncertainties=True)
+    assert singular.status[0] == 0 and singular.uncertainty_status[0] == 3
+    boundary = bf.fit(x, y, p0=[2, 0.2, 0.7], bounds=([2, -5, 0.01], [np.inf, 5, 5]), device="cuda",
+                      uncertainties=True)
+    assert boundary.uncertainty_status[0] == 4
+    noisy = y + np.random.default_rng(101).normal(0, 0.03, len(x))
+    fixed = bf.fit(x, noisy, p0=[2, 0.2, 0.7], bounds=([0, 0.2, 0.7], [np.inf, 0.2, 0.7]), device="cuda",
+                   uncertainties=True)
+    assert fixed.uncertainty_status[0] == 0
+    np.testing.assert_array_equal(fixed.covariance[0, 1:], 0)
+    np.testing.assert_array_equal(fixed.stderr[0, 1:], 0)
+    shape = 1 / (1 + ((x - 0.2) / 0.7) ** 2)
+    expected = fixed.chi2[0] / (len(x) - 1) / np.sum(shape ** 2)
+    np.testing.assert_allclose(fixed.covariance[0, 0, 0], expected, rtol=1e-5)
+    empty = bf.fit(x, np.empty((0, len(x))), device="cuda", uncertainties=True)
+    assert empty.covariance.shape == (0, 3, 3) and empty.stderr.shape == (0, 3)
+
+
+def test_uncertainty_does_not_change_fit(bf):
+    w = W.pseudo_voigt_plain(n=3000, seed=11)
+    a = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda")
+    b = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda", uncertainties=True)
+    for u, v in zip(a, b[:4]):
+        np.testing.assert_array_equal(u, v)
+    np.testing.assert_array_equal(b.covariance, b.covariance.transpose(0, 2, 1))
+
+
+@pytest.mark.parametrize("lanes", [8, 16, 32])
+def test_group_widths_agree(bf, lanes):
+    w = W.pseudo_voigt_plain(n=4000, seed=12)
+    base = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda", group_lanes=32)
+    r = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda", group_lanes=lanes)
+    agree = (r.status == base.status).mean()
+    assert agree >= 0.999
+    ok = (r.status == 0) & (base.status == 0)
+    pe = A.param_errors(w.model, w.x, w.y, r.params[ok], base.params[ok])
+    assert np.quantile(pe.max(1), 0.999) <= 1e-4
+
+
+def test_deterministic_and_position_independent(bf):
+    w = W.pseudo_voigt_plain(n=5000, seed=13)
+    a = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda", uncertainties=True)
+    b = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda", uncertainties=True)
+    for u, v in zip(a, b):
+        np.testing.assert_array_equal(u, v)
+    idx = np.array([0, 17, 4096, 4999])
+    c = bf.fit(w.x, w.y[idx], w.model, None, (w.lower, w.upper), "cuda", uncertainties=True)
+    for u, v in zip(a, c):
+        np.testing.assert_array_equal(u[idx], v)
+
+
+def test_device_memory_path_matches_host(bf):
+    import torch
+
+    w = W.pseudo_voigt_plain(n=3000, seed=14)
+    host = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda", uncertainties=True)
+    dev = bf.fit(torch.from_numpy(w.x).cuda(), torch.from_numpy(w.y).cuda(), w.model, None, (w.lower, w.upper),
+                 "cuda", uncertainties=True)
+    for u, v in zip(host, dev):
+        np.testing.assert_array_equal(u, v.cpu().numpy().astype(u.dtype))
+
+
+def test_empty_and_single(bf):
+    x = np.linspace(-4, 4, 129)
+    r = bf.fit(x, np.empty((0, 129)), device="cuda")
+    assert r.params.shape == (0, 3) and r.chi2.shape == (0,)
+    y = 2 / (1 + ((x - 0.2) / 0.7) ** 2)
+    r = bf.fit(x.tolist(), y.tolist(), p0=[1.8, 0, 0.8], device="cuda")
+    assert r.params.shape == (1, 3) and r.status[0] == 0
+    np.testing.assert_allclose(r.params[0], [2, 0.2, 0.7], atol=2e-4)
+
+
+def test_async_submit_wait(bf):
+    import ctypes as C
+
+    from batchfit_b200 import _capi
+
+    w = W.pseudo_voigt_plain(n=2000, seed=15)
+    ctx = bf.context(0)
+    n, p = w.y.shape[0], 4
+    params = np.empty((n, p), np.float32)
+    status = np.empty(n, np.int32)
+    iters = np.empty(n, np.uint32)
+    chi2 = np.empty(n, np.float32)
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    opts = bf.solver_options("pseudo_voigt", w.lower, w.upper)
+    args = _capi.FitArgs(2, n, w.x.size, ptr(w.x), ptr(w.y), None, _capi.BF_MEMORY_HOST, 0, 0, opts)
+    outs = _capi.FitOutputs(ptr(params), ptr(status), ptr(iters), ptr(chi2), None, None, None)
+    pending = ctx.submit(args, outs)
+    with pytest.raises(RuntimeError):
+        ctx.submit(args, outs)  # the context is busy until the wait
+    ctx.wait(pending)
+    ref = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda")
+    np.testing.assert_array_equal(params, ref.params)
+    t = ctx.timing()
+    assert t.launches >= 1 and t.kernel_ms > 0
