@@ -29,7 +29,7 @@ EXPORTS = (
     "bf_cuda_last_error", "bf_cuda_available", "bf_cuda_version", "bf_cuda_context_create",
     "bf_cuda_context_destroy", "bf_cuda_default_options", "bf_cuda_fit", "bf_cuda_submit", "bf_cuda_ready",
     "bf_cuda_wait", "bf_cuda_guess", "bf_cuda_last_timing", "bf_cuda_host_alloc", "bf_cuda_host_free",
-    "bf_cuda_max_points",
+    "bf_cuda_max_points", "bf_cuda_measure_peaks",
 )
 
 
@@ -77,6 +77,11 @@ class FitOutputs(C.Structure):
     ]
 
 
+class Peaks(C.Structure):
+    _fields_ = [("fp32_tflops", C.c_double), ("fp64_tflops", C.c_double), ("mufu_ex2_gops", C.c_double),
+                ("mufu_rcp_gops", C.c_double)]
+
+
 class Timing(C.Structure):
     _fields_ = [
         ("kernel_ms", C.c_double),
@@ -120,6 +125,7 @@ def load():
         lib.bf_cuda_host_free.argtypes = [vp]
         lib.bf_cuda_max_points.argtypes = [C.c_int32]
         lib.bf_cuda_max_points.restype = C.c_uint32
+        lib.bf_cuda_measure_peaks.argtypes = [vp, C.POINTER(Peaks)]
         for name in EXPORTS:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
         _lib = lib
@@ -190,6 +196,11 @@ class Context:
     def guess(self, model, n, m, x_ptr, y_ptr, memory, params_ptr, status_ptr):
         check(self._lib.bf_cuda_guess(self._ptr, model, n, m, x_ptr, y_ptr, memory, params_ptr, status_ptr),
               "bf_cuda_guess")
+
+    def measure_peaks(self) -> Peaks:
+        p = Peaks()
+        check(self._lib.bf_cuda_measure_peaks(self._ptr, C.byref(p)), "bf_cuda_measure_peaks")
+        return p
 
     def timing(self) -> Timing:
         t = Timing()

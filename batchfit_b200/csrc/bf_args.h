@@ -28,15 +28,13 @@ struct FitArgs {
     float lower[8], upper[8];
 };
 
-// Optional data-only guess outputs (testing and bf_cuda_guess).
-struct GuessArgs {
-    float *guesses;         // [N,P] or nullptr
-    int32_t *guess_status;  // [N] or nullptr
-    int guess_only;         // 1: stop after the guess
-};
-
 struct LaunchInfo {
     int grid, block, smem, blocks_per_sm, group_lanes;
+};
+
+// Measured pipe throughputs (roofline denominators).
+struct PeakRates {
+    double fp32_tflops, fp64_tflops, mufu_ex2_gops, mufu_rcp_gops;
 };
 
 } // namespace bf

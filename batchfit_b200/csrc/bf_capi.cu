@@ -65,8 +65,13 @@ struct DeviceBuffer {
 
 // Device-side storage of one in-flight chunk.
 struct Slot {
-    DeviceBuffer y, p0, params, status, iterations, chi2, cov, se, ustatus, counter;
-    cudaEvent_t k0 = nullptr, k1 = nullptr;
+    DeviceBuffer y, p0, guess, params, status, iterations, chi2, cov, se, ustatus, counter;
+};
+
+// Guess-only outputs (bf_cuda_guess); null members in a fit.
+struct GuessOnly {
+    float *params;
+    int32_t *status;
 };
 
 constexpr int kSlots = 2;
@@ -105,7 +110,7 @@ int choose_lanes(int model, uint32_t m, int requested) {
     if (lanes != 8 && lanes != 16 && lanes != 32) {
         // Points per lane between ~8 and ~32 keeps the group reduction and the FP64
         // control amortised without starving the scheduler of independent fits.
-        lanes = m <= 192 ? 8 : m <= 768 ? 16 : 32;
+        lanes = m <= 1024 ? 8 : m <= 2048 ? 16 : 32;
     }
     // Fewer, wider groups per CTA when the per-group spectrum buffers do not fit.
     while (lanes < 32 && bf::smem_bytes(model, lanes, int(m)) > kSmemLimit)
@@ -198,13 +203,49 @@ cudaEvent_t take_event(bf_cuda_context *ctx) {
     return e;
 }
 
-// Enqueue a whole fit on the context's streams.  Returns BF_OK once queued.
-int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &out, const bf::GuessArgs &guess_args) {
+// Launch the kernels of one batch already resident on the device: the data-only
+// guess when there are no initial values (into `guess_buf`), then the LM kernel.
+int launch_batch(bf_cuda_context *ctx, const bf_fit_args &in, const bf::FitArgs &base, int lanes, const float *x,
+                 const float *y, const float *p0, float *guess_buf, int32_t *guess_status, bool guess_only,
+                 const bf_fit_outputs &dev_out, unsigned long long *counter, long long count, cudaStream_t st) {
+    cudaEvent_t k0 = take_event(ctx), k1 = take_event(ctx);
+    BF_CUDA(cudaEventRecord(k0, st));
+    if (!p0 || guess_only) {
+        BF_CUDA(bf::launch_guess(in.model, lanes, x, y, count, int(in.m), guess_buf, guess_status, ctx->sms, st));
+        ++ctx->launches;
+        p0 = guess_buf;
+    }
+    if (!guess_only) {
+        bf::FitArgs a = base;
+        a.x = x;
+        a.y = y;
+        a.p0 = p0;
+        a.params = dev_out.params;
+        a.status = dev_out.status;
+        a.iterations = dev_out.iterations;
+        a.chi2 = dev_out.chi2;
+        a.covariance = dev_out.covariance;
+        a.stderr_out = dev_out.standard_errors;
+        a.ustatus = dev_out.uncertainty_status;
+        a.n = count;
+        a.work_counter = counter;
+        BF_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+        BF_CUDA(bf::launch_fit(in.model, lanes, a, ctx->sms, st, &ctx->info));
+        ++ctx->launches;
+    }
+    BF_CUDA(cudaEventRecord(k1, st));
+    ctx->kernel_events.push_back({k0, k1});
+    return BF_OK;
+}
+
+// Enqueue a whole fit (or guess-only run) on the context's streams.
+int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &out, const GuessOnly *guess_only) {
     const int p = parameter_count(in.model);
     const uint64_t n = in.n, m = in.m;
     const int lanes = choose_lanes(in.model, in.m, in.group_lanes);
     ctx->lanes = lanes;
     ctx->launches = 0;
+    ctx->info = bf::LaunchInfo{};
     for (auto &ev : ctx->kernel_events) {
         ctx->event_pool.push_back(ev.first);
         ctx->event_pool.push_back(ev.second);
@@ -213,36 +254,33 @@ int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &o
     BF_CUDA(cudaSetDevice(ctx->device));
     BF_CUDA(cudaEventRecord(ctx->start, ctx->stream[0]));
     BF_CUDA(cudaStreamWaitEvent(ctx->stream[1], ctx->start, 0));
-    bf::FitArgs base = make_args(in, p);
+    const bf::FitArgs base = make_args(in, p);
+    const bool need_guess = in.p0 == nullptr || guess_only != nullptr;
 
     if (in.memory == BF_MEMORY_DEVICE) {
         Slot &s = ctx->slot[0];
         BF_CUDA(s.counter.reserve(sizeof(unsigned long long)));
-        bf::FitArgs a = base;
-        a.x = in.x;
-        a.y = in.y;
-        a.p0 = in.p0;
-        a.params = out.params;
-        a.status = out.status;
-        a.iterations = out.iterations;
-        a.chi2 = out.chi2;
-        a.covariance = out.covariance;
-        a.stderr_out = out.standard_errors;
-        a.ustatus = out.uncertainty_status;
-        a.n = (long long)n;
-        a.work_counter = static_cast<unsigned long long *>(s.counter.ptr);
+        float *gbuf = nullptr;
+        int32_t *gstat = nullptr;
+        if (guess_only) {
+            gbuf = guess_only->params;
+            gstat = guess_only->status;
+        } else if (need_guess) {
+            BF_CUDA(s.guess.reserve(n * p * sizeof(float)));
+            gbuf = static_cast<float *>(s.guess.ptr);
+        }
         if (n > 0) {
-            BF_CUDA(cudaMemsetAsync(a.work_counter, 0, sizeof(unsigned long long), ctx->stream[0]));
-            cudaEvent_t k0 = take_event(ctx), k1 = take_event(ctx);
-            BF_CUDA(cudaEventRecord(k0, ctx->stream[0]));
-            BF_CUDA(bf::launch_fit(in.model, lanes, a, guess_args, ctx->sms, ctx->stream[0], &ctx->info));
-            BF_CUDA(cudaEventRecord(k1, ctx->stream[0]));
-            ctx->kernel_events.push_back({k0, k1});
-            ctx->launches = 1;
+            const int rc = launch_batch(ctx, in, base, lanes, in.x, in.y, in.p0, gbuf, gstat, guess_only != nullptr,
+                                        out, static_cast<unsigned long long *>(s.counter.ptr), (long long)n,
+                                        ctx->stream[0]);
+            if (rc != BF_OK)
+                return rc;
         }
         BF_CUDA(cudaEventRecord(ctx->stop, ctx->stream[0]));
         return BF_OK;
     }
+    if (guess_only)
+        return fail(BF_ERR_INVALID_ARGUMENT, "guess-only runs take device memory");
 
     // Host memory: x once, then double-buffered chunks.
     BF_CUDA(ctx->x.reserve(m * sizeof(float)));
@@ -261,6 +299,8 @@ int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &o
         BF_CUDA(s.y.reserve(chunk * m * sizeof(float)));
         if (has_p0)
             BF_CUDA(s.p0.reserve(chunk * p * sizeof(float)));
+        else
+            BF_CUDA(s.guess.reserve(chunk * p * sizeof(float)));
         BF_CUDA(s.params.reserve(chunk * p * sizeof(float)));
         BF_CUDA(s.status.reserve(chunk * sizeof(int32_t)));
         BF_CUDA(s.iterations.reserve(chunk * sizeof(uint32_t)));
@@ -281,26 +321,17 @@ int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &o
         if (has_p0)
             BF_CUDA(cudaMemcpyAsync(s.p0.ptr, in.p0 + first * p, count * p * sizeof(float), cudaMemcpyHostToDevice,
                                     st));
-        bf::FitArgs a = base;
-        a.x = static_cast<const float *>(ctx->x.ptr);
-        a.y = static_cast<const float *>(s.y.ptr);
-        a.p0 = has_p0 ? static_cast<const float *>(s.p0.ptr) : nullptr;
-        a.params = static_cast<float *>(s.params.ptr);
-        a.status = static_cast<int32_t *>(s.status.ptr);
-        a.iterations = static_cast<uint32_t *>(s.iterations.ptr);
-        a.chi2 = static_cast<float *>(s.chi2.ptr);
-        a.covariance = static_cast<float *>(s.cov.ptr);
-        a.stderr_out = static_cast<float *>(s.se.ptr);
-        a.ustatus = static_cast<int32_t *>(s.ustatus.ptr);
-        a.n = (long long)count;
-        a.work_counter = static_cast<unsigned long long *>(s.counter.ptr);
-        BF_CUDA(cudaMemsetAsync(a.work_counter, 0, sizeof(unsigned long long), st));
-        cudaEvent_t k0 = take_event(ctx), k1 = take_event(ctx);
-        BF_CUDA(cudaEventRecord(k0, st));
-        BF_CUDA(bf::launch_fit(in.model, lanes, a, guess_args, ctx->sms, st, &ctx->info));
-        BF_CUDA(cudaEventRecord(k1, st));
-        ctx->kernel_events.push_back({k0, k1});
-        ++ctx->launches;
+        const bf_fit_outputs dev_out{static_cast<float *>(s.params.ptr),     static_cast<int32_t *>(s.status.ptr),
+                                     static_cast<uint32_t *>(s.iterations.ptr), static_cast<float *>(s.chi2.ptr),
+                                     static_cast<float *>(s.cov.ptr),        static_cast<float *>(s.se.ptr),
+                                     static_cast<int32_t *>(s.ustatus.ptr)};
+        const int rc = launch_batch(ctx, in, base, lanes, static_cast<const float *>(ctx->x.ptr),
+                                    static_cast<const float *>(s.y.ptr),
+                                    has_p0 ? static_cast<const float *>(s.p0.ptr) : nullptr,
+                                    static_cast<float *>(s.guess.ptr), nullptr, false, dev_out,
+                                    static_cast<unsigned long long *>(s.counter.ptr), (long long)count, st);
+        if (rc != BF_OK)
+            return rc;
         auto d2h = [&](void *dst, const void *src, size_t bytes) {
             return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
         };
@@ -413,6 +444,7 @@ void bf_cuda_context_destroy(bf_cuda_context *ctx) {
     for (auto &s : ctx->slot) {
         s.y.release();
         s.p0.release();
+        s.guess.release();
         s.params.release();
         s.status.release();
         s.iterations.release();
@@ -478,7 +510,7 @@ int bf_cuda_submit(bf_cuda_context *ctx, const bf_fit_args *args, const bf_fit_o
         return fail(BF_ERR_BUSY, "a submission is already in flight on this context");
     {
         std::lock_guard<std::mutex> lock(ctx->mutex);
-        rc = enqueue(ctx, *args, *out, bf::GuessArgs{nullptr, nullptr, 0});
+        rc = enqueue(ctx, *args, *out, nullptr);
     }
     if (rc != BF_OK) {
         // Drain whatever was queued before the failure.
@@ -562,7 +594,8 @@ int bf_cuda_guess(bf_cuda_context *ctx, int32_t model, uint64_t n, uint32_t m, c
             break;
         if (memory == BF_MEMORY_DEVICE) {
             bf_fit_args a = args;
-            rc = enqueue(ctx, a, out, bf::GuessArgs{params, guess_status, 1});
+            const GuessOnly go{params, guess_status};
+            rc = enqueue(ctx, a, out, &go);
             if (rc == BF_OK)
                 rc = finish(ctx);
             break;
@@ -589,8 +622,8 @@ int bf_cuda_guess(bf_cuda_context *ctx, int32_t model, uint64_t n, uint32_t m, c
             a.x = static_cast<const float *>(dx.ptr);
             a.y = static_cast<const float *>(dy.ptr);
             a.memory = BF_MEMORY_DEVICE;
-            rc = enqueue(ctx, a, out,
-                         bf::GuessArgs{static_cast<float *>(dp.ptr), static_cast<int32_t *>(ds.ptr), 1});
+            const GuessOnly go{static_cast<float *>(dp.ptr), static_cast<int32_t *>(ds.ptr)};
+            rc = enqueue(ctx, a, out, &go);
             if (rc == BF_OK)
                 rc = finish(ctx);
             if (rc == BF_OK) {
@@ -614,6 +647,26 @@ int bf_cuda_last_timing(bf_cuda_context *ctx, bf_cuda_timing *out) {
     if (!ctx || !out)
         return fail(BF_ERR_INVALID_ARGUMENT, "null argument");
     *out = ctx->last;
+    return BF_OK;
+}
+
+int bf_cuda_measure_peaks(bf_cuda_context *ctx, bf_cuda_peaks *out) {
+    if (!ctx || !out)
+        return fail(BF_ERR_INVALID_ARGUMENT, "null argument");
+    if (ctx->busy.exchange(true))
+        return fail(BF_ERR_BUSY, "a submission is already in flight on this context");
+    std::lock_guard<std::mutex> lock(ctx->mutex);
+    bf::PeakRates rates{};
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess)
+        e = bf::measure_peaks(ctx->sms, ctx->stream[0], &rates);
+    ctx->busy.store(false);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "peak microbenchmarks");
+    out->fp32_tflops = rates.fp32_tflops;
+    out->fp64_tflops = rates.fp64_tflops;
+    out->mufu_ex2_gops = rates.mufu_ex2_gops;
+    out->mufu_rcp_gops = rates.mufu_rcp_gops;
     return BF_OK;
 }
 

@@ -1,14 +1,20 @@
-// Persistent fit kernels: one thread group (8, 16 or 32 lanes) per spectrum.
+// Fit kernels: one thread group (8, 16 or 32 lanes) per spectrum.
 //
-// Per CTA: the shared x grid is staged in shared memory once and its derived
-// constants (finiteness, monotone spacing, guess edge abscissae) computed there.
-// Per group: claim a fit (atomic work counter), stage its fit-major y row in
-// shared memory with 128-bit streaming loads, run the data-only guess when no
-// initial values are given, run bounded LM, and write the outputs.
+// guess_kernel: the data-only initial guess per spectrum (spectrum staged in
+//   shared memory, group-parallel searches), written to a [N,P] buffer.
+// lm_kernel: persistent bounded LM in rounds.  Every round each group runs exactly
+//   one fused pass for its fit -- the initial cost/linearisation of a newly
+//   claimed fit or the trial of an ongoing one -- then its FP64 control.  A group
+//   whose fit finished claims the next one (atomic work counter) at the start of
+//   the following round, so the groups of a warp stay in the same code (the pass)
+//   instead of drifting through different phases.
+//
+// Per CTA the shared x grid is staged in shared memory once and its derived
+// constants computed there.  Per group the fit-major y row is staged with 128-bit
+// streaming loads; group buffers are offset by G banks so the groups of a warp
+// read disjoint banks.
 #include "bf_kernels.h"
 #include "bf_lm.cuh"
-
-#include <cstdio>
 
 namespace bf {
 
@@ -24,38 +30,35 @@ __host__ __device__ inline int pow2_at_least(int v) {
     return p;
 }
 
-template <int MODEL> __host__ __device__ inline int group_smem_bytes(int m) {
-    const int n1 = pow2_at_least(edge_count(m));
-    int bytes = 4 * round_up(m, 4) + 4 * 2 * n1;
-    bytes = round_up(bytes, 16);
-    bytes += 2 * Layout<MODEL>::K * 8;
-    return round_up(bytes, 16);
-}
+// Per-group shared memory, in 4-byte words, padded so that consecutive groups of a
+// warp start G banks apart.
+__host__ __device__ inline int bank_staggered(int words, int lanes) { return round_up(words, 32) + (lanes % 32); }
 
-template <int MODEL, int G> int kernel_smem_bytes(int m) {
-    return 4 * round_up(m, 4) + (kBlock / G) * group_smem_bytes<MODEL>(m);
+template <int MODEL> __host__ __device__ inline int lm_group_words(int m, int lanes) {
+    return bank_staggered(round_up(m, 4) + 4 * Layout<MODEL>::K, lanes); // y row + 2 FP64 state slots
 }
+__host__ __device__ inline int guess_group_words(int m, int lanes) {
+    return bank_staggered(round_up(m, 4) + 2 * pow2_at_least(edge_count(m)), lanes); // y row + sort scratch
+}
+__host__ __device__ inline int x_words(int m) { return round_up(m, 4); }
 
-template <int MODEL, int G> __global__ void __launch_bounds__(kBlock, kMinBlocks) fit_kernel(FitArgs a, GuessArgs ga) {
-    constexpr int P = Model<MODEL>::P;
-    constexpr int kGroups = kBlock / G;
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ XConst xc;
+template <int MODEL, int G> int lm_smem_bytes(int m) { return 4 * (x_words(m) + (kBlock / G) * lm_group_words<MODEL>(m, G)); }
+template <int G> int guess_smem_bytes(int m) { return 4 * (x_words(m) + (kBlock / G) * guess_group_words(m, G)); }
+
+// CTA prologue: stage x and derive the grid constants (solver.hpp:58-69,223-239;
+// initial_guess.hpp:131-153).  Called by every thread of the block.
+__device__ void cta_prologue(const float *x, int m, float *xs, XConst &xc) {
     __shared__ unsigned int min_abs_bits, min_diff_bits;
-    const int m = a.m;
-    float *xs = reinterpret_cast<float *>(smem);
     const int tid = threadIdx.x;
-
-    // ---- CTA prologue: stage x and derive the grid constants. ----
     if (tid == 0) {
         min_abs_bits = 0x7f800000u;
         min_diff_bits = 0x7f800000u;
     }
-    for (int j = tid; j < m; j += kBlock)
-        xs[j] = a.x[j];
+    for (int j = tid; j < m; j += blockDim.x)
+        xs[j] = x[j];
     __syncthreads();
     bool fin = true, up = true, down = true, strict = true, varied = false;
-    for (int j = tid; j < m; j += kBlock) {
+    for (int j = tid; j < m; j += blockDim.x) {
         const float v = xs[j];
         fin = fin && isfinite(v);
         varied = varied || v != xs[0];
@@ -90,210 +93,411 @@ template <int MODEL, int G> __global__ void __launch_bounds__(kBlock, kMinBlocks
         xc.right_x = midpoint_rn(xs[m - count + (count - 1) / 2], xs[m - count + count / 2]);
     }
     __syncthreads();
+}
+
+// Stage one fit-major y row into shared memory; reports finiteness, flatness
+// (every value equal to y[0]) and sum(y^2).
+template <int G>
+__device__ __forceinline__ void stage_row(const Group<G> &g, const float *row, int m, bool vec_ok, float *ys,
+                                          bool &yfin, bool &flat, float &syy) {
+    const float y0 = __ldg(row);
+    yfin = true;
+    flat = true;
+    syy = 0.0f;
+    if (vec_ok) {
+        const float4 *row4 = reinterpret_cast<const float4 *>(row);
+        for (int v = int(g.lane); v < m / 4; v += G) {
+            const float4 t = __ldcs(row4 + v);
+            reinterpret_cast<float4 *>(ys)[v] = t;
+            yfin = yfin && isfinite(t.x) && isfinite(t.y) && isfinite(t.z) && isfinite(t.w);
+            flat = flat && t.x == y0 && t.y == y0 && t.z == y0 && t.w == y0;
+            syy = fmaf(t.x, t.x, fmaf(t.y, t.y, fmaf(t.z, t.z, fmaf(t.w, t.w, syy))));
+        }
+    } else {
+        for (int j = int(g.lane); j < m; j += G) {
+            const float t = __ldcs(row + j);
+            ys[j] = t;
+            yfin = yfin && isfinite(t);
+            flat = flat && t == y0;
+            syy = fmaf(t, t, syy);
+        }
+    }
+    yfin = g.all(yfin);
+    flat = g.all(flat);
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1)
+        syy += g.xor_(syy, o);
+    g.sync();
+}
+
+// ------------------------------------------------------------ guess kernel --
+template <int MODEL, int G>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) guess_kernel(const float *x, const float *y, long long n,
+                                                                   int m, float *guesses, int32_t *guess_status) {
+    constexpr int P = Model<MODEL>::P;
+    constexpr int kGroups = kBlock / G;
+    extern __shared__ __align__(16) float smem[];
+    __shared__ XConst xc;
+    float *xs = smem;
+    cta_prologue(x, m, xs, xc);
     const XConst cx = xc;
-
-    // ---- per-group buffers ----
     const Group<G> g;
-    const int gid = tid / G;
-    unsigned char *gbase = smem + 4 * round_up(m, 4) + gid * group_smem_bytes<MODEL>(m);
-    float *ys = reinterpret_cast<float *>(gbase);
+    const int gid = threadIdx.x / G;
+    float *ys = smem + x_words(m) + gid * guess_group_words(m, G);
     float *scratch = ys + round_up(m, 4);
-    double *state = reinterpret_cast<double *>(gbase + round_up(4 * round_up(m, 4) + 8 * cx.n1, 16));
-    const bool vec_ok = (m & 3) == 0 && (reinterpret_cast<uintptr_t>(a.y) & 15) == 0;
-
-    long long next_static = (long long)blockIdx.x * kGroups + gid;
-    while (true) {
-        long long fit;
-        if (a.work_counter) {
-            unsigned long long t = 0;
-            if (g.lane == 0)
-                t = atomicAdd(a.work_counter, 1ull);
-            fit = (long long)g.bcast(t, 0);
-        } else {
-            fit = next_static;
-            next_static += (long long)gridDim.x * kGroups;
-        }
-        if (fit >= a.n)
-            break;
-
-        // ---- stage y (fit-major row) ----
-        const float *row = a.y + fit * (long long)m;
-        const float y0 = __ldg(row);
-        bool yfin = true, flat = true;
-        float syy = 0.0f;
-        if (vec_ok) {
-            const float4 *row4 = reinterpret_cast<const float4 *>(row);
-            for (int v = int(g.lane); v < m / 4; v += G) {
-                const float4 t = __ldcs(row4 + v);
-                reinterpret_cast<float4 *>(ys)[v] = t;
-                yfin = yfin && isfinite(t.x) && isfinite(t.y) && isfinite(t.z) && isfinite(t.w);
-                flat = flat && t.x == y0 && t.y == y0 && t.z == y0 && t.w == y0;
-                syy = fmaf(t.x, t.x, fmaf(t.y, t.y, fmaf(t.z, t.z, fmaf(t.w, t.w, syy))));
-            }
-        } else {
-            for (int j = int(g.lane); j < m; j += G) {
-                const float t = __ldcs(row + j);
-                ys[j] = t;
-                yfin = yfin && isfinite(t);
-                flat = flat && t == y0;
-                syy = fmaf(t, t, syy);
-            }
-        }
-        yfin = g.all(yfin);
-        flat = g.all(flat);
-#pragma unroll
-        for (int o = G / 2; o >= 1; o >>= 1)
-            syy += g.xor_(syy, o);
-        g.sync();
-
-        // ---- initial values ----
+    const bool vec_ok = (m & 3) == 0 && (reinterpret_cast<uintptr_t>(y) & 15) == 0;
+    for (long long fit = (long long)blockIdx.x * kGroups + gid; fit < n; fit += (long long)gridDim.x * kGroups) {
+        bool yfin, flat;
+        float syy;
+        stage_row(g, y + fit * (long long)m, m, vec_ok, ys, yfin, flat, syy);
         float p[P];
-        if (a.p0) {
-#pragma unroll
-            for (int k = 0; k < P; ++k)
-                p[k] = __ldg(a.p0 + fit * P + k);
-        } else {
-            const int gs = initial_guess<MODEL, G>(g, cx, xs, ys, yfin, scratch, p);
-            if (ga.guesses) {
-#pragma unroll
-                for (int k = 0; k < P; ++k)
-                    if (int(g.lane) == k)
-                        ga.guesses[fit * P + k] = p[k];
-                if (g.lane == 0 && ga.guess_status)
-                    ga.guess_status[fit] = gs;
-            }
-        }
-        if (ga.guess_only) {
-            g.sync();
-            continue;
-        }
-
-        // ---- LM ----
-        int slot = 0;
-        const FitOutcome r = lm_solve<MODEL, G>(g, a, cx, xs, ys, yfin, flat, double(syy), p, state, slot);
-        const float chi2f = float(r.chi2);
+        const int gs = initial_guess<MODEL, G>(g, cx, xs, ys, yfin, scratch, p);
 #pragma unroll
         for (int k = 0; k < P; ++k)
             if (int(g.lane) == k)
-                a.params[fit * P + k] = p[k];
-        if (g.lane == 0) {
-            a.status[fit] = r.status;
-            a.iterations[fit] = r.iterations;
-            a.chi2[fit] = chi2f;
-        }
-        if (a.uncertainties) {
-            const int us = lm_uncertainty<MODEL, G>(g, a, cx, p, r.status, chi2f, state,
-                                                    state + slot * Layout<MODEL>::K, a.policy == kPolicyParity,
-                                                    a.covariance + fit * P * P, a.stderr_out + fit * P);
-            if (g.lane == 0)
-                a.ustatus[fit] = us;
-        }
+                guesses[fit * P + k] = p[k];
+        if (g.lane == 0 && guess_status)
+            guess_status[fit] = gs;
         g.sync();
     }
 }
 
-// ------------------------------------------------------------ host side --
-template <int MODEL, int G> static const void *kernel_ptr() {
-    return reinterpret_cast<const void *>(&fit_kernel<MODEL, G>);
+// --------------------------------------------------------------- LM kernel --
+template <int MODEL, int G>
+__device__ __forceinline__ void write_fit(const Group<G> &g, const FitArgs &a, long long fit, const LmState<MODEL> &s) {
+    constexpr int P = Model<MODEL>::P;
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        if (int(g.lane) == k)
+            a.params[fit * P + k] = s.p[k];
+    if (g.lane == 0) {
+        a.status[fit] = s.status;
+        a.iterations[fit] = s.iterations;
+        a.chi2[fit] = float(s.chi2);
+    }
 }
 
 template <int MODEL, int G>
-static cudaError_t launch_typed(const FitArgs &a, const GuessArgs &ga, int sms, cudaStream_t stream,
-                                LaunchInfo *info) {
-    const int smem = kernel_smem_bytes<MODEL, G>(a.m);
-    cudaError_t e = cudaFuncSetAttribute(kernel_ptr<MODEL, G>(), cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+__global__ void __launch_bounds__(kBlock, kMinBlocks) lm_kernel(FitArgs a) {
+    constexpr int P = Model<MODEL>::P;
+    constexpr int kGroups = kBlock / G;
+    extern __shared__ __align__(16) float smem[];
+    __shared__ XConst xc;
+    const int m = a.m;
+    float *xs = smem;
+    cta_prologue(a.x, m, xs, xc);
+    const XConst cx = xc;
+    const Group<G> g;
+    const int gid = threadIdx.x / G;
+    float *ys = smem + x_words(m) + gid * lm_group_words<MODEL>(m, G);
+    double *state = reinterpret_cast<double *>(ys + round_up(m, 4));
+    const bool vec_ok = (m & 3) == 0 && (reinterpret_cast<uintptr_t>(a.y) & 15) == 0;
+    const float qnan = __int_as_float(0x7fffffff);
+
+    long long next_static = (long long)blockIdx.x * kGroups + gid;
+    LmState<MODEL> s;
+    long long fit = -1;
+    bool flat = false;
+    float syy = 0.0f;
+    while (true) {
+        if (fit < 0) {
+            // Intake: claim fits until one needs a pass or the queue is empty.
+            while (true) {
+                long long f;
+                if (a.work_counter) {
+                    unsigned long long t = 0;
+                    if (g.lane == 0)
+                        t = atomicAdd(a.work_counter, 1ull);
+                    f = (long long)g.bcast(t, 0);
+                } else {
+                    f = next_static;
+                    next_static += (long long)gridDim.x * kGroups;
+                }
+                if (f >= a.n)
+                    break;
+                bool yfin;
+                stage_row(g, a.y + f * (long long)m, m, vec_ok, ys, yfin, flat, syy);
+                bool init_finite = true;
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    s.p[k] = __ldg(a.p0 + f * P + k);
+                    init_finite = init_finite && isfinite(s.p[k]);
+                }
+                if (a.options_ok && init_finite && cx.x_finite && yfin) {
+                    lm_begin<MODEL>(a, s);
+                    fit = f;
+                    break;
+                }
+                // Preflight rejection (solver.hpp:205-226): parameters keep the initial values.
+                s.status = kInvalid;
+                s.iterations = 0;
+                s.chi2 = __longlong_as_double(0x7ff8000000000000ll);
+                write_fit<MODEL, G>(g, a, f, s);
+                if (a.uncertainties) {
+                    for (int k = int(g.lane); k < P * P; k += G)
+                        a.covariance[f * P * P + k] = qnan;
+                    for (int k = int(g.lane); k < P; k += G)
+                        a.stderr_out[f * P + k] = qnan;
+                    if (g.lane == 0)
+                        a.ustatus[f] = kNotConverged;
+                }
+            }
+            if (fit < 0)
+                break;
+        }
+        lm_pass<MODEL, G>(g, xs, ys, m, s.t, state + (1 - s.cur) * Layout<MODEL>::K);
+        bool done = lm_after_pass<MODEL, G>(g, a, cx, flat, state, s);
+        if (!done)
+            done = lm_plan<MODEL>(a, cx, double(syy), state, s);
+        if (done) {
+            write_fit<MODEL, G>(g, a, fit, s);
+            if (a.uncertainties) {
+                const int us = lm_uncertainty<MODEL, G>(g, a, cx, s.p, s.status, float(s.chi2), state,
+                                                        state + s.cur * Layout<MODEL>::K, a.policy == kPolicyParity,
+                                                        a.covariance + fit * P * P, a.stderr_out + fit * P);
+                if (g.lane == 0)
+                    a.ustatus[fit] = us;
+            }
+            g.sync();
+            fit = -1;
+        }
+    }
+}
+
+// ------------------------------------------------ roofline microbenchmarks --
+// Throughput of the pipes the fit kernels are bound by, measured on the device the
+// fits run on: 8 independent dependency chains per thread, enough warps to cover
+// the pipe latency.  `sink` only keeps the chains alive.
+constexpr int kPeakChains = 8;
+
+__global__ void __launch_bounds__(256) peak_ffma_kernel(float *sink, int iters) {
+    float a[kPeakChains];
+#pragma unroll
+    for (int k = 0; k < kPeakChains; ++k)
+        a[k] = float(threadIdx.x + k) * 1e-3f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < kPeakChains; ++k)
+            a[k] = fmaf(a[k], 0.999999f, 1e-7f);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kPeakChains; ++k)
+        s += a[k];
+    if (s == -1.0f)
+        sink[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(256) peak_dfma_kernel(double *sink, int iters) {
+    double a[kPeakChains];
+#pragma unroll
+    for (int k = 0; k < kPeakChains; ++k)
+        a[k] = double(threadIdx.x + k) * 1e-3;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < kPeakChains; ++k)
+            a[k] = fma(a[k], 0.999999, 1e-7);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < kPeakChains; ++k)
+        s += a[k];
+    if (s == -1.0)
+        sink[blockIdx.x] = s;
+}
+
+template <bool EX2> __global__ void __launch_bounds__(256) peak_mufu_kernel(float *sink, int iters) {
+    float a[kPeakChains];
+#pragma unroll
+    for (int k = 0; k < kPeakChains; ++k)
+        a[k] = 0.5f + float(threadIdx.x + k) * 1e-4f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < kPeakChains; ++k)
+            a[k] = EX2 ? ex2_approx(-a[k]) : rcp_approx(a[k] + 1.0f);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kPeakChains; ++k)
+        s += a[k];
+    if (s == -1.0f)
+        sink[blockIdx.x] = s;
+}
+
+template <class F> static cudaError_t time_best(F launch, cudaStream_t s, float &best_ms) {
+    cudaEvent_t e0, e1;
+    cudaError_t e = cudaEventCreate(&e0);
     if (e != cudaSuccess)
         return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fit_kernel<MODEL, G>, kBlock, smem);
+    e = cudaEventCreate(&e1);
+    best_ms = 1e30f;
+    for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+        cudaEventRecord(e0, s);
+        launch();
+        cudaEventRecord(e1, s);
+        e = cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && ms < best_ms)
+            best_ms = ms; // first run is a warm-up
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
+cudaError_t measure_peaks(int sms, cudaStream_t s, PeakRates *out) {
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    void *sink = nullptr;
+    cudaError_t e = cudaMalloc(&sink, size_t(blocks) * sizeof(double));
+    if (e != cudaSuccess)
+        return e;
+    const double lanes = double(blocks) * threads * kPeakChains * iters;
+    float ms = 0.0f;
+    e = time_best([&] { peak_ffma_kernel<<<blocks, threads, 0, s>>>(static_cast<float *>(sink), iters); }, s, ms);
+    if (e == cudaSuccess)
+        out->fp32_tflops = 2.0 * lanes / (ms * 1e-3) / 1e12;
+    if (e == cudaSuccess)
+        e = time_best([&] { peak_dfma_kernel<<<blocks, threads, 0, s>>>(static_cast<double *>(sink), iters / 4); },
+                      s, ms);
+    if (e == cudaSuccess)
+        out->fp64_tflops = 2.0 * lanes / 4 / (ms * 1e-3) / 1e12;
+    if (e == cudaSuccess)
+        e = time_best([&] { peak_mufu_kernel<true><<<blocks, threads, 0, s>>>(static_cast<float *>(sink), iters / 4); },
+                      s, ms);
+    if (e == cudaSuccess)
+        out->mufu_ex2_gops = lanes / 4 / (ms * 1e-3) / 1e9;
+    if (e == cudaSuccess)
+        e = time_best(
+            [&] { peak_mufu_kernel<false><<<blocks, threads, 0, s>>>(static_cast<float *>(sink), iters / 4); }, s, ms);
+    if (e == cudaSuccess)
+        out->mufu_rcp_gops = lanes / 4 / (ms * 1e-3) / 1e9;
+    cudaFree(sink);
+    return e;
+}
+
+// ------------------------------------------------------------ host side --
+template <class K> static cudaError_t grid_for(K kernel, int smem, long long groups_needed, int groups_per_cta,
+                                               int sms, int &grid, int &per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void *>(kernel),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess)
+        return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, smem);
     if (e != cudaSuccess)
         return e;
     if (per_sm < 1)
         return cudaErrorInvalidConfiguration;
-    constexpr int groups = kBlock / G;
-    long long want = (a.n + groups - 1) / groups;
-    long long grid = (long long)per_sm * sms;
-    if (want < grid)
-        grid = want;
-    if (grid < 1)
-        grid = 1;
-    fit_kernel<MODEL, G><<<unsigned(grid), kBlock, smem, stream>>>(a, ga);
-    if (info) {
-        info->grid = int(grid);
-        info->block = kBlock;
-        info->smem = smem;
-        info->blocks_per_sm = per_sm;
-        info->group_lanes = G;
-    }
+    long long want = (groups_needed + groups_per_cta - 1) / groups_per_cta;
+    long long g = (long long)per_sm * sms;
+    if (want < g)
+        g = want;
+    grid = int(g < 1 ? 1 : g);
+    return cudaSuccess;
+}
+
+template <int MODEL, int G>
+static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t stream, LaunchInfo *info) {
+    const int smem = lm_smem_bytes<MODEL, G>(a.m);
+    int grid = 0, per_sm = 0;
+    cudaError_t e = grid_for(lm_kernel<MODEL, G>, smem, a.n, kBlock / G, sms, grid, per_sm);
+    if (e != cudaSuccess)
+        return e;
+    lm_kernel<MODEL, G><<<grid, kBlock, smem, stream>>>(a);
+    if (info)
+        *info = LaunchInfo{grid, kBlock, smem, per_sm, G};
+    return cudaGetLastError();
+}
+
+template <int MODEL, int G>
+static cudaError_t launch_guess_typed(const float *x, const float *y, long long n, int m, float *guesses,
+                                      int32_t *status, int sms, cudaStream_t stream) {
+    const int smem = guess_smem_bytes<G>(m);
+    int grid = 0, per_sm = 0;
+    cudaError_t e = grid_for(guess_kernel<MODEL, G>, smem, n, kBlock / G, sms, grid, per_sm);
+    if (e != cudaSuccess)
+        return e;
+    guess_kernel<MODEL, G><<<grid, kBlock, smem, stream>>>(x, y, n, m, guesses, status);
     return cudaGetLastError();
 }
 
 template <int MODEL>
-static cudaError_t launch_model(const FitArgs &a, const GuessArgs &ga, int lanes, int sms, cudaStream_t s,
-                                LaunchInfo *info) {
+static cudaError_t launch_lm_model(const FitArgs &a, int lanes, int sms, cudaStream_t s, LaunchInfo *info) {
     switch (lanes) {
-    case 8:
-        return launch_typed<MODEL, 8>(a, ga, sms, s, info);
-    case 16:
-        return launch_typed<MODEL, 16>(a, ga, sms, s, info);
-    default:
-        return launch_typed<MODEL, 32>(a, ga, sms, s, info);
+    case 8: return launch_lm_typed<MODEL, 8>(a, sms, s, info);
+    case 16: return launch_lm_typed<MODEL, 16>(a, sms, s, info);
+    default: return launch_lm_typed<MODEL, 32>(a, sms, s, info);
     }
 }
 
+template <int MODEL>
+static cudaError_t launch_guess_model(int lanes, const float *x, const float *y, long long n, int m, float *guesses,
+                                      int32_t *status, int sms, cudaStream_t s) {
+    switch (lanes) {
+    case 8: return launch_guess_typed<MODEL, 8>(x, y, n, m, guesses, status, sms, s);
+    case 16: return launch_guess_typed<MODEL, 16>(x, y, n, m, guesses, status, sms, s);
+    default: return launch_guess_typed<MODEL, 32>(x, y, n, m, guesses, status, sms, s);
+    }
+}
+
+cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStream_t s, LaunchInfo *info) {
+    switch (model) {
+    case kGaussian: return launch_lm_model<kGaussian>(a, lanes, sms, s, info);
+    case kLorentzian: return launch_lm_model<kLorentzian>(a, lanes, sms, s, info);
+    case kPseudoVoigt: return launch_lm_model<kPseudoVoigt>(a, lanes, sms, s, info);
+    case kTwoLorentzian: return launch_lm_model<kTwoLorentzian>(a, lanes, sms, s, info);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_guess(int model, int lanes, const float *x, const float *y, long long n, int m, float *guesses,
+                         int32_t *status, int sms, cudaStream_t s) {
+    switch (model) {
+    case kGaussian: return launch_guess_model<kGaussian>(lanes, x, y, n, m, guesses, status, sms, s);
+    case kLorentzian: return launch_guess_model<kLorentzian>(lanes, x, y, n, m, guesses, status, sms, s);
+    case kPseudoVoigt: return launch_guess_model<kPseudoVoigt>(lanes, x, y, n, m, guesses, status, sms, s);
+    case kTwoLorentzian: return launch_guess_model<kTwoLorentzian>(lanes, x, y, n, m, guesses, status, sms, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+int smem_bytes(int model, int lanes, int m) {
+    int lm = 0, gs = 0;
+    switch (model * 100 + lanes) {
+    case 8: lm = lm_smem_bytes<0, 8>(m); break;
+    case 16: lm = lm_smem_bytes<0, 16>(m); break;
+    case 32: lm = lm_smem_bytes<0, 32>(m); break;
+    case 108: lm = lm_smem_bytes<1, 8>(m); break;
+    case 116: lm = lm_smem_bytes<1, 16>(m); break;
+    case 132: lm = lm_smem_bytes<1, 32>(m); break;
+    case 208: lm = lm_smem_bytes<2, 8>(m); break;
+    case 216: lm = lm_smem_bytes<2, 16>(m); break;
+    case 232: lm = lm_smem_bytes<2, 32>(m); break;
+    case 308: lm = lm_smem_bytes<3, 8>(m); break;
+    case 316: lm = lm_smem_bytes<3, 16>(m); break;
+    default: lm = lm_smem_bytes<3, 32>(m); break;
+    }
+    switch (lanes) {
+    case 8: gs = guess_smem_bytes<8>(m); break;
+    case 16: gs = guess_smem_bytes<16>(m); break;
+    default: gs = guess_smem_bytes<32>(m); break;
+    }
+    return lm > gs ? lm : gs;
+}
+
 int max_points(int model) {
-    // Largest M whose per-CTA layout (x plus one 32-lane group... kBlock/32 groups) fits
-    // the 227 KB opt-in shared memory of one CTA.
+    // Largest M whose 32-lane layouts (guess and LM) fit one CTA's 227 KB.
     const int limit = 227 * 1024;
     int lo = 1, hi = 1 << 20;
     while (lo < hi) {
         const int mid = (lo + hi + 1) / 2;
-        int bytes = 0;
-        switch (model) {
-        case 0: bytes = kernel_smem_bytes<0, 32>(mid); break;
-        case 1: bytes = kernel_smem_bytes<1, 32>(mid); break;
-        case 2: bytes = kernel_smem_bytes<2, 32>(mid); break;
-        default: bytes = kernel_smem_bytes<3, 32>(mid); break;
-        }
-        if (bytes <= limit)
+        if (smem_bytes(model, 32, mid) <= limit)
             lo = mid;
         else
             hi = mid - 1;
     }
     return lo;
-}
-
-int smem_bytes(int model, int lanes, int m) {
-    switch (model * 100 + lanes) {
-    case 8: return kernel_smem_bytes<0, 8>(m);
-    case 16: return kernel_smem_bytes<0, 16>(m);
-    case 32: return kernel_smem_bytes<0, 32>(m);
-    case 108: return kernel_smem_bytes<1, 8>(m);
-    case 116: return kernel_smem_bytes<1, 16>(m);
-    case 132: return kernel_smem_bytes<1, 32>(m);
-    case 208: return kernel_smem_bytes<2, 8>(m);
-    case 216: return kernel_smem_bytes<2, 16>(m);
-    case 232: return kernel_smem_bytes<2, 32>(m);
-    case 308: return kernel_smem_bytes<3, 8>(m);
-    case 316: return kernel_smem_bytes<3, 16>(m);
-    default: return kernel_smem_bytes<3, 32>(m);
-    }
-}
-
-cudaError_t launch_fit(int model, int lanes, const FitArgs &a, const GuessArgs &ga, int sms, cudaStream_t s,
-                       LaunchInfo *info) {
-    switch (model) {
-    case kGaussian:
-        return launch_model<kGaussian>(a, ga, lanes, sms, s, info);
-    case kLorentzian:
-        return launch_model<kLorentzian>(a, ga, lanes, sms, s, info);
-    case kPseudoVoigt:
-        return launch_model<kPseudoVoigt>(a, ga, lanes, sms, s, info);
-    case kTwoLorentzian:
-        return launch_model<kTwoLorentzian>(a, ga, lanes, sms, s, info);
-    default:
-        return cudaErrorInvalidValue;
-    }
 }
 
 } // namespace bf

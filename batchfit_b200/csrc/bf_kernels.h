@@ -5,15 +5,22 @@
 
 namespace bf {
 
-// Launch the persistent fit kernel for `model` with `lanes` (8, 16 or 32) lanes per
-// fit on `stream`.  The caller zeroes a.work_counter (when non-null) beforehand.
-cudaError_t launch_fit(int model, int lanes, const FitArgs &a, const GuessArgs &ga, int sms,
-                       cudaStream_t stream, LaunchInfo *info);
+// Launch the persistent LM kernel for `model` with `lanes` (8, 16 or 32) lanes per
+// fit on `stream`.  a.p0 must hold initial values for every fit (the user's, or the
+// guess kernel's output).  The caller zeroes a.work_counter (when non-null) first.
+cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStream_t stream, LaunchInfo *info);
+
+// Launch the data-only guess kernel: guesses[N*P] and, when non-null, status[N].
+cudaError_t launch_guess(int model, int lanes, const float *x, const float *y, long long n, int m, float *guesses,
+                         int32_t *status, int sms, cudaStream_t stream);
 
 // Dynamic shared memory of one CTA for (model, lanes, M).
 int smem_bytes(int model, int lanes, int m);
 
 // Largest M the shared-memory layout supports for `model`.
 int max_points(int model);
+
+// FP32 FMA, FP64 FMA and MUFU ex2/rcp throughput on the current device.
+cudaError_t measure_peaks(int sms, cudaStream_t stream, PeakRates *out);
 
 } // namespace bf

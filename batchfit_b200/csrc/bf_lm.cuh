@@ -200,77 +200,128 @@ template <int MODEL> __device__ __forceinline__ int spectral_success(const float
     return kConverged;
 }
 
-struct FitOutcome {
+// Per-fit LM state carried between rounds (registers).  The accepted J^T J, J^T r
+// and chi2 live in shared-memory slot `cur`; a pass writes slot 1 - cur.
+template <int MODEL> struct LmState {
+    static constexpr int P = Model<MODEL>::P;
+    float p[P];       // accepted parameters (reported)
+    float t[P];       // point of the next pass: the projected initial values or a trial
+    double chi2;      // accepted objective
+    double lambda, lambda_max, predicted;
+    uint32_t it;         // iteration index (solver.hpp:254)
+    uint32_t iterations; // reported attempted updates (solver.hpp:287)
     int status;
-    uint32_t iterations;
-    double chi2;
+    int cur;
+    bool initial; // the next pass is the fit's initial cost + linearisation
 };
 
-// The LM iteration proper (fit_single after the input copy).  `p` enters as the
-// initial values and leaves as the reported parameters.  `state` holds two
-// K-slot FP64 state blocks in shared memory.
+// Start a fit whose inputs passed preflight: project the initial values into the
+// bounds (solver.hpp:227-229); the first pass evaluates there.
+template <int MODEL> __device__ __forceinline__ void lm_begin(const FitArgs &a, LmState<MODEL> &s) {
+#pragma unroll
+    for (int k = 0; k < Model<MODEL>::P; ++k) {
+        s.p[k] = sclamp(s.p[k], a.lower[k], a.upper[k]);
+        s.t[k] = s.p[k];
+    }
+    s.initial = true;
+    s.cur = 0;
+    s.it = 0;
+    s.iterations = 0;
+    s.status = kMaxIterations;
+}
+
+// Consume the pass that just wrote slot 1 - s.cur.  Returns true when the fit is
+// finished (s.status final).
 template <int MODEL, int G>
-__device__ FitOutcome lm_solve(const Group<G> &g, const FitArgs &a, const XConst &xc, const float *xs,
-                               const float *ys, bool y_finite, bool y_flat, double syy, float (&p)[Model<MODEL>::P],
-                               double *state, int &cur_slot) {
+__device__ __forceinline__ bool lm_after_pass(const Group<G> &g, const FitArgs &a, const XConst &xc, bool y_flat,
+                                              const double *state, LmState<MODEL> &s) {
+    using L = Layout<MODEL>;
+    const double c = state[(1 - s.cur) * L::K];
+    if (s.initial) {
+        // Initial cost and linearisation (solver.hpp:230-253).
+        s.initial = false;
+        if (!isfinite(c)) {
+            s.status = kInvalid;
+            s.chi2 = __longlong_as_double(0x7ff8000000000000ll);
+            return true;
+        }
+        s.chi2 = c;
+        if (xc.varied_x && y_flat && free_shape<MODEL>(a)) {
+            s.status = kDegenerate;
+            return true;
+        }
+        s.cur = 1 - s.cur;
+        s.lambda = a.lambda0;
+        s.lambda_max = fmax(a.lambda0, 1.0 / kFltEps);
+        return false;
+    }
+    // Accept / reject the trial and update lambda (solver.hpp:313-339).
+    const double reduction = s.chi2 - c;
+    const double threshold = a.ftol * s.chi2;
+    const bool small = isfinite(c) && isfinite(s.predicted) && s.predicted >= 0.0 && fabs(reduction) <= threshold &&
+                       s.predicted <= threshold / fmax(1.0, s.lambda);
+    if (isfinite(c) && reduction > 0.0 && isfinite(s.predicted) && s.predicted > 0.0) {
+#pragma unroll
+        for (int k = 0; k < Model<MODEL>::P; ++k)
+            s.p[k] = s.t[k];
+        s.chi2 = c;
+        s.cur = 1 - s.cur;
+        const double ratio = reduction / s.predicted;
+        const double u = 2.0 * ratio - 1.0;
+        const double factor = ratio >= 1.0 ? 1.0 / 3.0 : fmax(1.0 / 3.0, 1.0 - u * u * u);
+        s.lambda = dclamp(s.lambda * factor, a.policy == kPolicyParity ? kDblEps : kFltEps, s.lambda_max);
+    } else {
+        s.lambda = fmin(s.lambda_max, s.lambda * 10.0);
+    }
+    // The next pass overwrites the slot just read.
+    g.sync();
+    s.it += 1;
+    if (small) {
+        s.status = spectral_success<MODEL>(s.p, xc.spacing);
+        return true;
+    }
+    return false;
+}
+
+// Plan the next trial from the accepted state (solver.hpp:254-312).  Returns true
+// when the fit finished instead; otherwise s.t holds the next pass point.
+template <int MODEL>
+__device__ __forceinline__ bool lm_plan(const FitArgs &a, const XConst &xc, double syy, const double *state,
+                                        LmState<MODEL> &s) {
     using L = Layout<MODEL>;
     constexpr int P = L::P;
-    FitOutcome out{kInvalid, 0u, __longlong_as_double(0x7ff8000000000000ll)};
-    const int m = xc.m;
-    bool init_finite = true;
-#pragma unroll
-    for (int k = 0; k < P; ++k)
-        init_finite = init_finite && isfinite(p[k]);
-    if (!a.options_ok || !init_finite || !xc.x_finite || !y_finite)
-        return out;
-#pragma unroll
-    for (int k = 0; k < P; ++k)
-        p[k] = sclamp(p[k], a.lower[k], a.upper[k]);
-    double *cur = state + cur_slot * L::K;
-    lm_pass<MODEL, G>(g, xs, ys, m, p, cur);
-    double chi2 = cur[0];
-    if (!isfinite(chi2))
-        return out;
-    out.chi2 = chi2;
-    if (xc.varied_x && y_flat && free_shape<MODEL>(a)) {
-        out.status = kDegenerate;
-        return out;
-    }
     const bool parity = a.policy == kPolicyParity;
-    const double eps_t = parity ? kDblEps : kFltEps;
-    double lambda = a.lambda0;
-    const double lambda_max = fmax(a.lambda0, 1.0 / kFltEps);
-    out.status = kMaxIterations;
-    const double floor_g = a.noise_floor * kFltEps * sqrt(syy);
-    for (uint32_t it = 0; it < a.max_iterations; ++it) {
-        // Accepted-state finiteness (the reference's linearize() check).  A and g
-        // stay in shared memory; lanes read them as broadcasts when needed.
+    while (true) {
+        if (s.it >= a.max_iterations)
+            return true; // status stays max_iterations
+        const double *cur = state + s.cur * L::K;
         const double *A = cur + 1 + P; // packed lower triangle
         const double *gr = cur + 1;
         bool finite = true;
 #pragma unroll
-        for (int i = 0; i < L::K - 1; ++i)
-            finite = finite && isfinite(cur[1 + i]);
+        for (int i = 1; i < L::K; ++i)
+            finite = finite && isfinite(cur[i]);
         if (!finite) {
-            out.status = kInvalid;
-            break;
+            s.status = kInvalid;
+            return true;
         }
         bool active[P];
         double gnorm = 0.0;
         bool at_floor = true;
+        const double floor_g = a.noise_floor * kFltEps * sqrt(syy);
 #pragma unroll
         for (int k = 0; k < P; ++k) {
             const double gk = gr[k];
-            active[k] = a.lower[k] == a.upper[k] || (p[k] == a.lower[k] && gk < 0.0) ||
-                        (p[k] == a.upper[k] && gk > 0.0);
+            active[k] = a.lower[k] == a.upper[k] || (s.p[k] == a.lower[k] && gk < 0.0) ||
+                        (s.p[k] == a.upper[k] && gk > 0.0);
             if (!active[k]) {
                 gnorm = fmax(gnorm, fabs(gk));
                 at_floor = at_floor && fabs(gk) <= floor_g * sqrt(fmax(A[k * (k + 1) / 2 + k], 0.0));
             }
         }
         if (gnorm <= a.gtol || (parity && at_floor)) {
-            out.status = spectral_success<MODEL>(p, xc.spacing);
-            break;
+            s.status = spectral_success<MODEL>(s.p, xc.spacing);
+            return true;
         }
         double D[P * (P + 1) / 2], delta[P];
 #pragma unroll
@@ -282,31 +333,30 @@ __device__ FitOutcome lm_solve(const Group<G> &g, const FitArgs &a, const XConst
                 if (active[k] || active[l])
                     v = 0.0;
                 if (k == l)
-                    v = active[k] ? 1.0 : v + lambda * A[k * (k + 1) / 2 + k];
+                    v = active[k] ? 1.0 : v + s.lambda * A[k * (k + 1) / 2 + k];
                 D[k * (k + 1) / 2 + l] = v;
             }
         }
-        out.iterations = it + 1;
+        s.iterations = s.it + 1;
         if (!chol_solve<P>(D, delta, (a.flags & kFlagScaledCholesky) != 0u)) {
-            out.status = kSingular;
-            break;
+            s.status = kSingular;
+            return true;
         }
-        float trial[P];
         double step_norm = 0.0, param_norm = 0.0;
         bool finite_trial = true;
 #pragma unroll
         for (int k = 0; k < P; ++k) {
             step_norm = fmax(step_norm, fabs(delta[k]));
-            trial[k] = float(dclamp(double(p[k]) + delta[k], double(a.lower[k]), double(a.upper[k])));
-            finite_trial = finite_trial && isfinite(trial[k]);
-            delta[k] = double(trial[k]) - double(p[k]);
-            param_norm = fmax(param_norm, fabs(double(p[k])));
+            s.t[k] = float(dclamp(double(s.p[k]) + delta[k], double(a.lower[k]), double(a.upper[k])));
+            finite_trial = finite_trial && isfinite(s.t[k]);
+            delta[k] = double(s.t[k]) - double(s.p[k]);
+            param_norm = fmax(param_norm, fabs(double(s.p[k])));
         }
-        const double damp = fmax(1.0, lambda);
+        const double damp = fmax(1.0, s.lambda);
         if (step_norm <= a.xtol * (param_norm + a.xtol) / damp ||
             (parity && step_norm * damp <= a.step_quantum * kFltEps * param_norm)) {
-            out.status = spectral_success<MODEL>(p, xc.spacing);
-            break;
+            s.status = spectral_success<MODEL>(s.p, xc.spacing);
+            return true;
         }
         double predicted = 0.0;
 #pragma unroll
@@ -318,39 +368,13 @@ __device__ FitOutcome lm_solve(const Group<G> &g, const FitArgs &a, const XConst
                 predicted -= delta[k] * akl * delta[l];
             }
         }
-        double trial_cost = __longlong_as_double(0x7ff8000000000000ll);
-        double *nxt = state + (1 - cur_slot) * L::K;
-        if (finite_trial) {
-            lm_pass<MODEL, G>(g, xs, ys, m, trial, nxt);
-            trial_cost = nxt[0];
-        }
-        const double reduction = chi2 - trial_cost;
-        const double threshold = a.ftol * chi2;
-        const bool small = isfinite(trial_cost) && isfinite(predicted) && predicted >= 0.0 &&
-                           fabs(reduction) <= threshold && predicted <= threshold / damp;
-        if (isfinite(trial_cost) && reduction > 0.0 && isfinite(predicted) && predicted > 0.0) {
-#pragma unroll
-            for (int k = 0; k < P; ++k)
-                p[k] = trial[k];
-            chi2 = trial_cost;
-            cur_slot = 1 - cur_slot;
-            cur = nxt;
-            const double ratio = reduction / predicted;
-            const double u = 2.0 * ratio - 1.0;
-            const double factor = ratio >= 1.0 ? 1.0 / 3.0 : fmax(1.0 / 3.0, 1.0 - u * u * u);
-            lambda = dclamp(lambda * factor, eps_t, lambda_max);
-        } else {
-            lambda = fmin(lambda_max, lambda * 10.0);
-        }
-        // Every lane must finish reading `nxt` before a later pass overwrites it.
-        g.sync();
-        if (small) {
-            out.status = spectral_success<MODEL>(p, xc.spacing);
-            break;
-        }
+        s.predicted = predicted;
+        if (finite_trial)
+            return false;
+        // A non-finite trial has a NaN cost: rejected without evaluation.
+        s.lambda = fmin(s.lambda_max, s.lambda * 10.0);
+        s.it += 1;
     }
-    out.chi2 = chi2;
-    return out;
 }
 
 // Covariance from the accepted state's information matrix, FP64 inverse

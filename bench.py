@@ -1,0 +1,416 @@
+"""Benchmark: batched bounded-LM pseudo-Voigt fitting on B200.
+
+Workload (one step): 1,000,000 pseudo-Voigt fits (amplitude, center, FWHM,
+mixing) at M=512 on x = linspace(-10, 10, 512), float32, data-only guesses on the
+GPU (p0=None), bounds [0,-10,1e-3,0]/[inf,10,10,1], uncertainties=True.  Seeded
+synthetic spectra with the configuration's distributions (A~U[0.5,5], c~U[-6,6],
+FWHM~logU[0.1,3], mixing~U[0,1], noise sigma = 1% of A).  y is 2.048 GB per GPU,
+larger than L2 (126 MB), so no L2 flush is needed between steps.
+
+* value     fits/s with x, y resident in HBM (one fit-kernel launch per step).
+* e2e       the same fits through the C ABI from pinned host buffers: host->device
+            copies, kernels and device->host result copies inside each step.
+* accuracy  a 20,000-fit sample of the step's outputs against the float64 oracle.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+N > 1 is launched under torch.distributed.run: every rank fits its own batch
+(weak scaling, no data-path collective); time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fits/s at ≤1e-4 rel err vs FP64; p50/p99 latency, served vs plain on one B200"
+MODEL, M, P = "pseudo_voigt", 512, 4
+WORKLOAD = "pseudo_voigt_plain: 1M pseudo-Voigt fits, M=512, float32, p0=None, uncertainties=True"
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM bytes of one fit-kernel launch per fit, from the committed ncu capture of the
+# same kernel (profiles/fit_kernel_pv512.md): traffic scales with the fits processed.
+TRAFFIC_BYTES_PER_FIT = None
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("cuda", "reference"), default="cuda")
+    ap.add_argument("--fits", type=int, default=1_000_000, help="fits per GPU per step")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- helpers --
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "cuda" else "gloo"
+        if backend == "nccl":
+            import torch
+
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(value, world, device=None):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sms, maxes, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                maxes.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sms:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxes), "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def measured_peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+# ------------------------------------------------------------- CPU legs --
+def cpu_reference_rate(w, seconds_budget, dtype=np.float32):
+    """The reference's own CPU path (oracle/_ref: guesses + cpu::fit_batch with
+    uncertainties) on all host threads, over a bounded sample of the workload."""
+    from oracle import pyoracle
+
+    if pyoracle.ref_available():
+        kind, run = "reference", lambda n: pyoracle.fit("ref", MODEL, w.x, w.y[:n], None, w.lower, w.upper, dtype,
+                                                        uncertainties=True)
+        cores = int(pyoracle.load_ref().bfref_hardware_concurrency())
+    else:
+        kind, run = "port", lambda n: pyoracle.fit("port", MODEL, w.x, w.y[:n], None, w.lower, w.upper, dtype,
+                                                   uncertainties=True)
+        cores = 1
+    n = min(2000, w.y.shape[0])
+    t0 = time.perf_counter()
+    run(n)  # warm-up and size probe
+    per_fit = (time.perf_counter() - t0) / n
+    n = int(min(w.y.shape[0], max(n, seconds_budget / 3 / max(per_fit, 1e-9))))
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        run(n)
+        times.append(time.perf_counter() - t0)
+    sec = statistics.median(times)
+    return {"value": n / sec, "unit": "fits/s", "cores": cores, "kind": kind,
+            "sample": f"{n} fits of the same workload ({np.dtype(dtype).name} reference path incl. data-only guesses "
+                      f"and covariance), median of 3 after a warm-up"}
+
+
+def accuracy_sample(w, res_np, n=20000):
+    from batchfit_b200 import accuracy
+    from oracle import pyoracle
+
+    n = min(n, w.y.shape[0])
+    impl = "ref" if pyoracle.ref_available() else "port"
+    ref = pyoracle.fit(impl, MODEL, w.x, w.y[:n], None, w.lower, w.upper, np.float64, uncertainties=True)
+    counted = pyoracle.fit("port", MODEL, w.x, w.y[:2000], None, w.lower, w.upper, np.float64, count_passes=True)
+    s = accuracy.summarize(MODEL, w.x, w.y[:n], res_np["params"][:n], res_np["status"][:n], res_np["chi2"][:n],
+                           ref.params, ref.status, ref.chi2)
+    us_agree = float((res_np["ustatus"][:n] == ref.uncertainty_status).mean())
+    c = counted.counters
+    passes = {"linearize": c.linearize_passes / 2000, "cost": c.cost_passes / 2000, "iterations": c.iterations / 2000}
+    return {"oracle": f"float64 reference CPU path ({impl}) on the first {n} fits",
+            "status_agreement": round(s["status_agreement"], 6),
+            "within_tol_fraction": round(s["within_tol_fraction"], 6),
+            "chi2_within_fraction": round(s["chi2_within_fraction"], 6),
+            "param_err_max": s["param_err_max"], "param_err_p999": s["param_err_p999"],
+            "chi2_err_max": s["chi2_err_max"], "uncertainty_status_agreement": round(us_agree, 6),
+            "param_tol": 1e-4, "chi2_tol": 1e-5}, passes
+
+
+# -------------------------------------------------------------- arms --
+def run_reference_arm(args, world, rank):
+    from batchfit_b200 import workloads
+
+    if rank != 0:
+        return 0
+    n = 200_000
+    w = workloads.pseudo_voigt_plain(n=n)
+    from oracle import pyoracle
+
+    impl = "ref" if pyoracle.ref_available() else "port"
+    cores = int(pyoracle.load_ref().bfref_hardware_concurrency()) if impl == "ref" else 1
+    # Size each step to a bounded sample of the workload (~1-2 s of CPU work).
+    probe = 2000
+    t0 = time.perf_counter()
+    pyoracle.fit(impl, MODEL, w.x, w.y[:probe], None, w.lower, w.upper, np.float32, uncertainties=True)
+    per_fit = (time.perf_counter() - t0) / probe
+    sample = int(min(n, max(probe, 1.5 / max(per_fit, 1e-9))))
+    for _ in range(args.warmup):
+        pyoracle.fit(impl, MODEL, w.x, w.y[:sample], None, w.lower, w.upper, np.float32, uncertainties=True)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        pyoracle.fit(impl, MODEL, w.x, w.y[:sample], None, w.lower, w.upper, np.float32, uncertainties=True)
+        times.append(time.perf_counter() - t0)
+    value = sample * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "fits_per_step": sample, "points": M, "model": MODEL,
+                   "sample": "bounded sample of the same workload per step"},
+        "cpu_baseline": {"value": value, "unit": "fits/s", "cores": cores,
+                         "kind": "reference" if impl == "ref" else "port",
+                         "sample": f"{sample} fits per step: the reference's float32 cpu::fit_batch with data-only "
+                                   f"guesses and uncertainties on {cores} host threads"},
+        "e2e": {"value": value, "unit": "fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_cuda_arm(args, world, rank, local):
+    import ctypes as C
+
+    import torch
+
+    import batchfit_b200 as bf
+    from batchfit_b200 import _capi, roofline, workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = workloads.pseudo_voigt_plain(n=args.fits, seed=2 + rank)
+    n = w.y.shape[0]
+    ctx = bf.context(local)
+    opts = bf.solver_options(MODEL, w.lower, w.upper, "parity")
+    x_d = torch.from_numpy(w.x).to(dev)
+    y_d = torch.from_numpy(w.y).to(dev)
+    out_d = {"params": torch.empty((n, P), dtype=torch.float32, device=dev),
+             "status": torch.empty(n, dtype=torch.int32, device=dev),
+             "iters": torch.empty(n, dtype=torch.int32, device=dev),
+             "chi2": torch.empty(n, dtype=torch.float32, device=dev),
+             "cov": torch.empty((n, P, P), dtype=torch.float32, device=dev),
+             "se": torch.empty((n, P), dtype=torch.float32, device=dev),
+             "ustatus": torch.empty(n, dtype=torch.int32, device=dev)}
+    dp = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    d_args = _capi.FitArgs(2, n, M, dp(x_d), dp(y_d), None, _capi.BF_MEMORY_DEVICE, 1, 0, opts)
+    d_outs = _capi.FitOutputs(dp(out_d["params"]), dp(out_d["status"]), dp(out_d["iters"]), dp(out_d["chi2"]),
+                              dp(out_d["cov"]), dp(out_d["se"]), dp(out_d["ustatus"]))
+    torch.cuda.synchronize()
+
+    # ---- value: device-resident inputs ----
+    for _ in range(args.warmup):
+        ctx.fit(d_args, d_outs)
+    barrier(world)
+    torch.cuda.synchronize()
+    step_ms, kernel_ms, launches = [], [], 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            ctx.fit(d_args, d_outs)
+            t = ctx.timing()
+            step_ms.append(t.total_ms)
+            kernel_ms.append(t.kernel_ms)
+            launches += t.launches
+            lanes, grid, bps = t.group_lanes, t.grid, t.blocks_per_sm
+    torch.cuda.synchronize()
+    barrier(world)
+    total_ms = max_over_ranks(sum(step_ms), world, dev)
+    value = world * n * args.steps / (total_ms * 1e-3)
+
+    # ---- e2e: pinned host buffers through the C ABI ----
+    lib = _capi.load()
+    host = {}
+
+    def pinned(nbytes):
+        ptr = C.c_void_p()
+        _capi.check(lib.bf_cuda_host_alloc(nbytes, C.byref(ptr)), "bf_cuda_host_alloc")
+        host[ptr.value] = nbytes
+        return ptr
+
+    hx, hy = pinned(w.x.nbytes), pinned(w.y.nbytes)
+    C.memmove(hx, w.x.ctypes.data, w.x.nbytes)
+    C.memmove(hy, w.y.ctypes.data, w.y.nbytes)
+    o_bytes = {"params": n * P * 4, "status": n * 4, "iters": n * 4, "chi2": n * 4, "cov": n * P * P * 4,
+               "se": n * P * 4, "ustatus": n * 4}
+    ho = {k: pinned(v) for k, v in o_bytes.items()}
+    h_args = _capi.FitArgs(2, n, M, hx, hy, None, _capi.BF_MEMORY_HOST, 1, 0, opts)
+    h_outs = _capi.FitOutputs(ho["params"], ho["status"], ho["iters"], ho["chi2"], ho["cov"], ho["se"],
+                              ho["ustatus"])
+    for _ in range(max(1, args.warmup)):
+        ctx.fit(h_args, h_outs)
+    barrier(world)
+    e2e_ms = []
+    for _ in range(args.steps):
+        ctx.fit(h_args, h_outs)
+        e2e_ms.append(ctx.timing().total_ms)
+    barrier(world)
+    e2e_total = max_over_ranks(sum(e2e_ms), world, dev)
+    e2e_value = world * n * args.steps / (e2e_total * 1e-3)
+    h2d = w.x.nbytes + w.y.nbytes
+    d2h = sum(o_bytes.values())
+
+    # Host and device paths must agree bit for bit.
+    res_np = {k: np.ctypeslib.as_array(C.cast(ho[k], C.POINTER(C.c_uint8)), (o_bytes[k],)).copy()
+              for k in o_bytes}
+    res_np = {"params": res_np["params"].view(np.float32).reshape(n, P),
+              "status": res_np["status"].view(np.int32), "chi2": res_np["chi2"].view(np.float32),
+              "ustatus": res_np["ustatus"].view(np.int32)}
+    same = bool(np.array_equal(res_np["params"], out_d["params"].cpu().numpy(), equal_nan=True))
+    for ptr in list(host):
+        lib.bf_cuda_host_free(C.c_void_p(ptr))
+
+    if rank != 0:
+        return 0
+    # ---- accuracy, roofline, CPU baseline (rank 0) ----
+    acc, passes = accuracy_sample(w, res_np)
+    peaks = ctx.measure_peaks()
+    flops, mufu = roofline.fit_work(MODEL, M, passes["linearize"], passes["cost"], True)
+    k_ms = statistics.mean(kernel_ms)
+    achieved_tf = flops * n / (k_ms * 1e-3) / 1e12
+    mufu_rate = mufu * n / (k_ms * 1e-3) / 1e9
+    mufu_peak = min(peaks.mufu_ex2_gops, peaks.mufu_rcp_gops)
+    ideal_ms = max(flops * n / (peaks.fp32_tflops * 1e12), mufu * n / (mufu_peak * 1e9),
+                   roofline.observation_bytes(M, P, True) * n / (measured_peaks().get("hbm_gbs", 6650.0) * 1e9)) * 1e3
+    hbm_gbs = roofline.observation_bytes(M, P, True) * n / (k_ms * 1e-3) / 1e9
+    mp = measured_peaks()
+    roof = {
+        "bound": "fp32", "achieved": round(achieved_tf, 3), "peak": round(peaks.fp32_tflops, 3), "unit": "TFLOP/s",
+        "frac": round(achieved_tf / peaks.fp32_tflops, 4),
+        "traffic": None if TRAFFIC_BYTES_PER_FIT is None else int(TRAFFIC_BYTES_PER_FIT * n),
+        "peak_source": "measured in this run: FFMA dependent-chain microbenchmark on this GPU (bf_cuda_measure_peaks)",
+        "ideal_ms": round(ideal_ms, 4), "kernel_ms": round(k_ms, 4),
+        "roofline_frac": round(ideal_ms / k_ms, 4),
+        "mufu": {"achieved_gops": round(mufu_rate, 1), "peak_gops": round(mufu_peak, 1),
+                 "frac": round(mufu_rate / mufu_peak, 4)},
+        "hbm": {"achieved": round(hbm_gbs, 1), "peak": mp.get("hbm_gbs"), "unit": "GB/s",
+                "frac": round(hbm_gbs / mp["hbm_gbs"], 4) if mp.get("hbm_gbs") else None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "work": {"flops_per_fit": round(flops), "mufu_per_fit": round(mufu), "oracle_passes": passes},
+    }
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = cpu_reference_rate(w, args.cpu_seconds)
+    lat = sorted(step_ms)
+    line = {
+        "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "fits_per_gpu": n, "points": M, "model": MODEL, "uncertainties": True,
+                   "p0": "None (GPU data-only guesses)", "policy": "parity", "group_lanes": lanes, "grid": grid,
+                   "blocks_per_sm": bps, "l2": "inputs (2.048 GB/GPU) exceed L2; no flush",
+                   "parallelism": f"replicas x{world} (independent fits, no collective)"},
+        "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, math.ceil(0.99 * len(lat)) - 1)],
+                       "what": "per-step (1M-fit batch) device time"},
+        "e2e": {"value": e2e_value, "unit": "fits/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "host_device_match": same},
+        "gpu_launches": launches,
+        "accuracy": acc,
+        "roofline": roof,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+        "peaks_measured": {"fp32_tflops": round(peaks.fp32_tflops, 2), "fp64_tflops": round(peaks.fp64_tflops, 2),
+                           "mufu_ex2_gops": round(peaks.mufu_ex2_gops, 1),
+                           "mufu_rcp_gops": round(peaks.mufu_rcp_gops, 1)},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            return run_reference_arm(args, world, rank)
+        return run_cuda_arm(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

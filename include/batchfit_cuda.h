@@ -151,6 +151,17 @@ int bf_cuda_host_free(void *ptr);
 /* Largest M the kernels support for `model` (shared-memory layout bound). */
 uint32_t bf_cuda_max_points(int32_t model);
 
+/* Roofline denominators measured on the context's device: dependent-chain
+ * throughput of FP32 FMA (2 flops each), FP64 FMA, and the MUFU ex2 / rcp
+ * approximations.  No reference counterpart (the reference has no roofline). */
+typedef struct bf_cuda_peaks {
+    double fp32_tflops;
+    double fp64_tflops;
+    double mufu_ex2_gops;
+    double mufu_rcp_gops;
+} bf_cuda_peaks;
+int bf_cuda_measure_peaks(bf_cuda_context *ctx, bf_cuda_peaks *out);
+
 #ifdef __cplusplus
 }
 #endif
