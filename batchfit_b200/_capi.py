@@ -29,7 +29,7 @@ EXPORTS = (
     "bf_cuda_last_error", "bf_cuda_available", "bf_cuda_version", "bf_cuda_context_create",
     "bf_cuda_context_destroy", "bf_cuda_default_options", "bf_cuda_fit", "bf_cuda_submit", "bf_cuda_ready",
     "bf_cuda_wait", "bf_cuda_guess", "bf_cuda_last_timing", "bf_cuda_host_alloc", "bf_cuda_host_free",
-    "bf_cuda_max_points", "bf_cuda_measure_peaks",
+    "bf_cuda_max_points", "bf_cuda_measure_peaks", "bf_cuda_fit_noalloc",
 )
 
 
@@ -126,6 +126,7 @@ def load():
         lib.bf_cuda_max_points.argtypes = [C.c_int32]
         lib.bf_cuda_max_points.restype = C.c_uint32
         lib.bf_cuda_measure_peaks.argtypes = [vp, C.POINTER(Peaks)]
+        lib.bf_cuda_fit_noalloc.argtypes = [C.POINTER(FitArgs), C.POINTER(FitOutputs), vp]
         for name in EXPORTS:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
         _lib = lib

@@ -372,6 +372,23 @@ int finish(bf_cuda_context *ctx) {
 
 } // namespace
 
+// Shared with bf_noalloc.cu: argument checks, kernel arguments and the group width
+// of a device-memory fit, and the thread-local error report.
+namespace bf {
+namespace host {
+int prepare(const bf_fit_args *args, const bf_fit_outputs *out, FitArgs *base, int *lanes) {
+    const int rc = validate(args, out);
+    if (rc != BF_OK)
+        return rc;
+    *base = make_args(*args, parameter_count(args->model));
+    *lanes = choose_lanes(args->model, args->m, args->group_lanes);
+    return BF_OK;
+}
+int report(int code, const std::string &message) { return fail(code, message); }
+int report_cuda(cudaError_t e, const char *what) { return cuda_fail(e, what); }
+} // namespace host
+} // namespace bf
+
 extern "C" {
 
 const char *bf_cuda_last_error(void) { return g_last_error.c_str(); }

@@ -151,6 +151,26 @@ int bf_cuda_host_free(void *ptr);
 /* Largest M the kernels support for `model` (shared-memory layout bound). */
 uint32_t bf_cuda_max_points(int32_t model);
 
+/* A fit that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: a host whose memory pool already owns
+ * the whole device, a real-time pipeline that reserves every buffer up front and
+ * forbids allocation while it runs, or a library callback that may only enqueue
+ * work on a stream it was given.  Every pointer in `args` and `out` is device
+ * memory of the current device (args->memory must be BF_MEMORY_DEVICE); the work
+ * is enqueued on `stream` (a cudaStream_t; NULL = the default stream) and the call
+ * returns without waiting -- synchronise the stream before reading the outputs.
+ * The kernels' only scratch (the work counter and the data-only guesses) lives in
+ * a 4 MiB static device array that every GPU loading this library holds until the
+ * process exits.  With p0 == NULL, N is limited to the guesses that fit it --
+ * 349,504 fits for P=3, 262,128 for P=4, 131,064 for P=8 -- and larger N is
+ * rejected with BF_ERR_INVALID_ARGUMENT; with p0 given, N is not limited.  The
+ * first call on a device resolves the array's device address (once per device)
+ * and should come before any stream capture.  All calls share the array: calls
+ * whose work overlaps on the GPU race, so serialise them (one stream, or wait
+ * between calls).  No context is needed. */
+int bf_cuda_fit_noalloc(const bf_fit_args *args, const bf_fit_outputs *out, void *stream);
+
 /* Roofline denominators measured on the context's device: dependent-chain
  * throughput of FP32 FMA (2 flops each), FP64 FMA, and the MUFU ex2 / rcp
  * approximations.  No reference counterpart (the reference has no roofline). */
