@@ -231,7 +231,7 @@ int launch_batch(bf_cuda_context *ctx, const bf_fit_args &in, const bf::FitArgs 
         a.work_counter = counter;
         BF_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
         BF_CUDA(bf::launch_fit(in.model, lanes, a, ctx->sms, st, &ctx->info));
-        ++ctx->launches;
+        ctx->launches += in.uncertainties ? 2 : 1; // LM kernel (+ covariance kernel)
     }
     BF_CUDA(cudaEventRecord(k1, st));
     ctx->kernel_events.push_back({k0, k1});

@@ -28,15 +28,18 @@ struct XConst {
 };
 
 // Ascending bitonic sort of `batches` consecutive arrays of n (power of two) floats.
+// Index arithmetic is shifts and masks only (n is a power of two).
 template <int G>
 __device__ __forceinline__ void bitonic_sort(const Group<G> &g, float *buf, int n, int batches) {
+    const int half_shift = 31 - __clz(n > 1 ? n >> 1 : 1);
+    const int half_mask = (n >> 1) - 1;
     const int pairs = (n >> 1) * batches;
     for (int k = 2; k <= n; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
             for (int t = int(g.lane); t < pairs; t += G) {
-                const int b = t / (n >> 1), u = t % (n >> 1);
+                const int b = t >> half_shift, u = t & half_mask;
                 const int i = ((u & ~(j - 1)) << 1) | (u & (j - 1));
-                float *a = buf + b * n;
+                float *a = buf + (b << (half_shift + 1));
                 const float lo = a[i], hi = a[i | j];
                 const bool ascending = (i & k) == 0;
                 if (ascending ? (lo > hi) : (lo < hi)) {
@@ -244,9 +247,10 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         return kGuessInvalid;
     const int m = xc.m, count = xc.count, n1 = xc.n1;
     // Edge medians (initial_guess.hpp:142-150).
+    const int n1_mask = n1 - 1;
     for (int t = int(g.lane); t < 2 * n1; t += G) {
-        const int side = t / n1, j = t % n1;
-        scratch[t] = j < count ? ys[side ? m - count + j : j] : __int_as_float(0x7f800000);
+        const int j = t & n1_mask;
+        scratch[t] = j < count ? ys[t >= n1 ? m - count + j : j] : __int_as_float(0x7f800000);
     }
     g.sync();
     bitonic_sort(g, scratch, n1, 2);

@@ -192,8 +192,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) lm_kernel(FitArgs a) {
     float *ys = smem + x_words(m) + gid * lm_group_words<MODEL>(m, G);
     double *state = reinterpret_cast<double *>(ys + round_up(m, 4));
     const bool vec_ok = (m & 3) == 0 && (reinterpret_cast<uintptr_t>(a.y) & 15) == 0;
-    const float qnan = __int_as_float(0x7fffffff);
-
     long long next_static = (long long)blockIdx.x * kGroups + gid;
     LmState<MODEL> s;
     long long fit = -1;
@@ -233,35 +231,60 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) lm_kernel(FitArgs a) {
                 s.iterations = 0;
                 s.chi2 = __longlong_as_double(0x7ff8000000000000ll);
                 write_fit<MODEL, G>(g, a, f, s);
-                if (a.uncertainties) {
-                    for (int k = int(g.lane); k < P * P; k += G)
-                        a.covariance[f * P * P + k] = qnan;
-                    for (int k = int(g.lane); k < P; k += G)
-                        a.stderr_out[f * P + k] = qnan;
-                    if (g.lane == 0)
-                        a.ustatus[f] = kNotConverged;
-                }
             }
             if (fit < 0)
                 break;
         }
-        lm_pass<MODEL, G>(g, xs, ys, m, s.t, state + (1 - s.cur) * Layout<MODEL>::K);
-        bool done = lm_after_pass<MODEL, G>(g, a, cx, flat, state, s);
+        const bool pass_finite = lm_pass<MODEL, G>(g, xs, ys, m, s.t, state + (1 - s.cur) * Layout<MODEL>::K);
+        bool done = lm_after_pass<MODEL, G>(g, a, cx, flat, pass_finite, state, s);
         if (!done)
             done = lm_plan<MODEL>(a, cx, double(syy), state, s);
         if (done) {
             write_fit<MODEL, G>(g, a, fit, s);
-            if (a.uncertainties) {
-                const int us = lm_uncertainty<MODEL, G>(g, a, cx, s.p, s.status, float(s.chi2), state,
-                                                        state + s.cur * Layout<MODEL>::K, a.policy == kPolicyParity,
-                                                        a.covariance + fit * P * P, a.stderr_out + fit * P);
-                if (g.lane == 0)
-                    a.ustatus[fit] = us;
+            if (a.uncertainties && s.status == kConverged) {
+                // The accepted J^T J (the information matrix at the reported
+                // parameters) for covariance_kernel, in the covariance output.
+                const double *cur = state + s.cur * Layout<MODEL>::K;
+                for (int k = int(g.lane); k < P * P; k += G) {
+                    const int i = k / P, j = k % P;
+                    a.covariance[fit * P * P + k] = float(cur[Layout<MODEL>::tri(i > j ? i : j, i > j ? j : i)]);
+                }
             }
             g.sync();
             fit = -1;
         }
     }
+}
+
+// ------------------------------------------------------- covariance kernel --
+// One thread per fit: reads the status, parameters, chi2 and the information
+// matrix the LM kernel left in the covariance output; writes covariance, standard
+// errors and the uncertainty status.
+constexpr int kCovBlock = 128;
+
+template <int MODEL> __global__ void __launch_bounds__(kCovBlock) covariance_kernel(FitArgs a) {
+    constexpr int P = Model<MODEL>::P;
+    const long long fit = (long long)blockIdx.x * kCovBlock + threadIdx.x;
+    if (fit >= a.n)
+        return;
+    float p[P], info[P * P], se[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        p[k] = a.params[fit * P + k];
+    const int status = a.status[fit];
+    if (status == kConverged) {
+#pragma unroll
+        for (int k = 0; k < P * P; ++k)
+            info[k] = a.covariance[fit * P * P + k];
+    }
+    const int us = covariance_one<MODEL>(a, p, status, a.chi2[fit], info, se);
+#pragma unroll
+    for (int k = 0; k < P * P; ++k)
+        a.covariance[fit * P * P + k] = info[k];
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        a.stderr_out[fit * P + k] = se[k];
+    a.ustatus[fit] = us;
 }
 
 // ------------------------------------------------ roofline microbenchmarks --
@@ -407,6 +430,10 @@ static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t strea
     lm_kernel<MODEL, G><<<grid, kBlock, smem, stream>>>(a);
     if (info)
         *info = LaunchInfo{grid, kBlock, smem, per_sm, G};
+    e = cudaGetLastError();
+    if (e != cudaSuccess || !a.uncertainties || a.n == 0)
+        return e;
+    covariance_kernel<MODEL><<<unsigned((a.n + kCovBlock - 1) / kCovBlock), kCovBlock, 0, stream>>>(a);
     return cudaGetLastError();
 }
 

@@ -6,8 +6,9 @@
 namespace bf {
 
 // Launch the persistent LM kernel for `model` with `lanes` (8, 16 or 32) lanes per
-// fit on `stream`.  a.p0 must hold initial values for every fit (the user's, or the
-// guess kernel's output).  The caller zeroes a.work_counter (when non-null) first.
+// fit on `stream`, followed by the covariance kernel when a.uncertainties.  a.p0
+// must hold initial values for every fit (the user's, or the guess kernel's
+// output).  The caller zeroes a.work_counter (when non-null) first.
 cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStream_t stream, LaunchInfo *info);
 
 // Launch the data-only guess kernel: guesses[N*P] and, when non-null, status[N].

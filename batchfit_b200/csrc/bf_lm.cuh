@@ -53,32 +53,40 @@ template <int MODEL> struct Layout {
 
 // Points a lane accumulates naively before folding chi2 and J^T r into its
 // compensated running sums.
-constexpr int kChunk = 8;
+constexpr int kChunk = 4;
 
 // One fused pass at parameters p: state[0] = chi2, state[1..P] = J^T r,
-// state[tri(k,l)] = (J^T J)_kl, as FP64 values.
+// state[tri(k,l)] = (J^T J)_kl, as FP64 values.  Returns whether all of them are
+// finite (the reference's linearize() check, solver.hpp:182-190, plus chi2).
 //
 // Accumulation: each lane sums kChunk points naively, then folds the chunk's chi2
 // and J^T r into Kahan pairs (numerics::add, numerics.hpp:12-18); the pairs enter
-// the group's two-sum tree with their low parts.  J^T r decides where the
-// iteration stops (its error moves the fixed point), so it gets the compensation;
-// J^T J only shapes the step and keeps plain per-lane sums.
+// a two-sum reduce-scatter across the group with their low parts.  J^T r decides
+// where the iteration stops (its error moves the fixed point), so it gets the
+// compensation; J^T J only shapes the step and takes a plain reduce-scatter.
 template <int MODEL, int G>
-__device__ __forceinline__ void lm_pass(const Group<G> &g, const float *xs, const float *ys, int m,
+__device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, const float *ys, int m,
                                         const float *p, double *state) {
     using L = Layout<MODEL>;
     constexpr int P = L::P;
+    constexpr int KC = P + 1;                 // chi2 and J^T r
+    constexpr int KCP = pow2ceil(KC);
+    constexpr int T = P * (P + 1) / 2;        // J^T J lower triangle
+    constexpr int TP = pow2ceil(T);
     const auto q = Model<MODEL>::prepare(p);
-    float hi[L::KP], lo[L::KP];
+    float hi[KCP], lo[KCP], aa[TP];
 #pragma unroll
-    for (int i = 0; i < L::KP; ++i) {
+    for (int i = 0; i < KCP; ++i) {
         hi[i] = 0.0f;
         lo[i] = 0.0f;
     }
-    for (int base = int(g.lane); base < m; base += G * kChunk) {
-        float part[1 + P];
 #pragma unroll
-        for (int i = 0; i <= P; ++i)
+    for (int i = 0; i < TP; ++i)
+        aa[i] = 0.0f;
+    for (int base = int(g.lane); base < m; base += G * kChunk) {
+        float part[KC];
+#pragma unroll
+        for (int i = 0; i < KC; ++i)
             part[i] = 0.0f;
 #pragma unroll
         for (int c = 0; c < kChunk; ++c) {
@@ -93,21 +101,24 @@ __device__ __forceinline__ void lm_pass(const Group<G> &g, const float *xs, cons
                     part[1 + k] = fmaf(J[k], r, part[1 + k]);
 #pragma unroll
                     for (int l = 0; l <= k; ++l)
-                        hi[L::tri(k, l)] = fmaf(J[k], J[l], hi[L::tri(k, l)]);
+                        aa[k * (k + 1) / 2 + l] = fmaf(J[k], J[l], aa[k * (k + 1) / 2 + l]);
                 }
             }
         }
         // Kahan fold; lo holds minus the Kahan correction, so the value is hi + lo.
 #pragma unroll
-        for (int i = 0; i <= P; ++i) {
+        for (int i = 0; i < KC; ++i) {
             const float adjusted = __fadd_rn(part[i], lo[i]);
             const float next = __fadd_rn(hi[i], adjusted);
             lo[i] = __fsub_rn(adjusted, __fsub_rn(next, hi[i]));
             hi[i] = next;
         }
     }
-    reduce_scatter_store<G, L::KP>(g, hi, lo, state, L::K);
+    bool finite = reduce_scatter_store<G, KCP>(g, hi, lo, state, KC);
+    finite = reduce_scatter_store_plain<G, TP>(g, aa, state + KC, T) && finite;
+    finite = g.all(finite);
     g.sync();
+    return finite;
 }
 
 // In-place Cholesky of a packed lower triangle (FP64) and solve of rhs.
@@ -212,7 +223,8 @@ template <int MODEL> struct LmState {
     uint32_t iterations; // reported attempted updates (solver.hpp:287)
     int status;
     int cur;
-    bool initial; // the next pass is the fit's initial cost + linearisation
+    bool initial;    // the next pass is the fit's initial cost + linearisation
+    bool cur_finite; // the accepted slot's chi2, J^T r and J^T J are all finite
 };
 
 // Start a fit whose inputs passed preflight: project the initial values into the
@@ -234,7 +246,7 @@ template <int MODEL> __device__ __forceinline__ void lm_begin(const FitArgs &a, 
 // finished (s.status final).
 template <int MODEL, int G>
 __device__ __forceinline__ bool lm_after_pass(const Group<G> &g, const FitArgs &a, const XConst &xc, bool y_flat,
-                                              const double *state, LmState<MODEL> &s) {
+                                              bool pass_finite, const double *state, LmState<MODEL> &s) {
     using L = Layout<MODEL>;
     const double c = state[(1 - s.cur) * L::K];
     if (s.initial) {
@@ -251,6 +263,7 @@ __device__ __forceinline__ bool lm_after_pass(const Group<G> &g, const FitArgs &
             return true;
         }
         s.cur = 1 - s.cur;
+        s.cur_finite = pass_finite;
         s.lambda = a.lambda0;
         s.lambda_max = fmax(a.lambda0, 1.0 / kFltEps);
         return false;
@@ -266,6 +279,7 @@ __device__ __forceinline__ bool lm_after_pass(const Group<G> &g, const FitArgs &
             s.p[k] = s.t[k];
         s.chi2 = c;
         s.cur = 1 - s.cur;
+        s.cur_finite = pass_finite;
         const double ratio = reduction / s.predicted;
         const double u = 2.0 * ratio - 1.0;
         const double factor = ratio >= 1.0 ? 1.0 / 3.0 : fmax(1.0 / 3.0, 1.0 - u * u * u);
@@ -297,11 +311,7 @@ __device__ __forceinline__ bool lm_plan(const FitArgs &a, const XConst &xc, doub
         const double *cur = state + s.cur * L::K;
         const double *A = cur + 1 + P; // packed lower triangle
         const double *gr = cur + 1;
-        bool finite = true;
-#pragma unroll
-        for (int i = 1; i < L::K; ++i)
-            finite = finite && isfinite(cur[i]);
-        if (!finite) {
+        if (!s.cur_finite) {
             s.status = kInvalid;
             return true;
         }
@@ -377,159 +387,155 @@ __device__ __forceinline__ bool lm_plan(const FitArgs &a, const XConst &xc, doub
     }
 }
 
-// Covariance from the accepted state's information matrix, FP64 inverse
-// (uncertainty.hpp:12-110), written to cov_out[P*P], se_out[P] (global memory).
-// `state` is the group's two-slot block; `cur` points at the accepted slot.  The
-// inverse columns are staged in `state` (both slots) once H sits in registers.
-template <int MODEL, int G>
-__device__ int lm_uncertainty(const Group<G> &g, const FitArgs &a, const XConst &xc,
-                              const float (&p)[Model<MODEL>::P], int fit_status, float chi2f, double *state,
-                              const double *cur, bool parity, float *cov_out, float *se_out) {
-    using L = Layout<MODEL>;
-    constexpr int P = L::P;
-    constexpr int T = P * (P + 1) / 2;
+// Covariance of one converged fit (include/batchfit/cpu/uncertainty.hpp:12-110),
+// one thread per fit.  `info` holds the accepted state's J^T J (P*P floats, the LM
+// kernel writes it into the caller's covariance output); it is replaced by the
+// covariance.  The inverse is FP64: one equilibrated Cholesky factorisation and P
+// triangular solves (the reference refactors per column with the same result).
+template <int MODEL>
+__device__ int covariance_one(const FitArgs &a, const float *p, int fit_status, float chi2f, float *info,
+                              float *se_out) {
+    constexpr int P = Model<MODEL>::P;
+    const float qnan = __int_as_float(0x7fffffff);
     int status = kAvailable;
     bool fixed[P];
     int nfree = 0;
-    double H[T];
-    double scale[P], inv[P];
-    double variance = 0.0;
     if (fit_status != kConverged)
         status = kNotConverged;
     else if (!isfinite(chi2f) || chi2f < 0.0f)
         status = kUInvalid;
-    if (status == kAvailable) {
 #pragma unroll
-        for (int k = 0; k < P; ++k) {
-            if (status != kAvailable)
-                break;
-            if (!isfinite(p[k]) || isnan(a.lower[k]) || isnan(a.upper[k]) || a.lower[k] > a.upper[k] ||
-                p[k] < a.lower[k] || p[k] > a.upper[k]) {
-                status = kUInvalid;
-                break;
-            }
-            fixed[k] = a.lower[k] == a.upper[k];
-            nfree += fixed[k] ? 0 : 1;
-            if (!fixed[k] && (p[k] == a.lower[k] || p[k] == a.upper[k]))
-                status = kActiveBound;
-        }
+    for (int k = 0; k < P; ++k) {
+        fixed[k] = a.lower[k] == a.upper[k];
+        nfree += fixed[k] ? 0 : 1;
+        if (status != kAvailable)
+            continue;
+        if (!isfinite(p[k]) || isnan(a.lower[k]) || isnan(a.upper[k]) || a.lower[k] > a.upper[k] ||
+            p[k] < a.lower[k] || p[k] > a.upper[k])
+            status = kUInvalid;
+        else if (!fixed[k] && (p[k] == a.lower[k] || p[k] == a.upper[k]))
+            status = kActiveBound;
     }
-    if (status == kAvailable && xc.m <= nfree)
+    if (status == kAvailable && a.m <= nfree)
         status = kInsufficientDof;
-    if (status == kAvailable && !xc.x_finite)
-        status = kUInvalid;
+    double H[P * (P + 1) / 2];
+    double inv[P];
     if (status == kAvailable) {
 #pragma unroll
         for (int k = 0; k < P; ++k)
 #pragma unroll
             for (int l = 0; l <= k; ++l) {
-                double v = cur[L::tri(k, l)];
+                double v = double(info[k * P + l]);
                 if (!isfinite(v))
                     status = kUInvalid;
                 if (fixed[k] || fixed[l])
                     v = (k == l) ? 1.0 : 0.0;
                 H[k * (k + 1) / 2 + l] = v;
             }
-        variance = double(chi2f) / double(xc.m - nfree);
-        if (!isfinite(variance))
-            status = kUInvalid;
     }
+    const double variance = double(chi2f) / double(a.m - nfree);
+    if (status == kAvailable && !isfinite(variance))
+        status = kUInvalid;
     if (status == kAvailable) {
-        // One equilibrated factorisation; the reference refactors per column with
-        // the same deterministic result.
 #pragma unroll
         for (int i = 0; i < P; ++i) {
             const double d = H[i * (i + 1) / 2 + i];
             if (!isfinite(d) || d <= 0.0)
                 status = kUSingular;
-            scale[i] = sqrt(d);
-        }
-        if (status == kAvailable) {
-#pragma unroll
-            for (int i = 0; i < P; ++i)
-#pragma unroll
-                for (int j = 0; j <= i; ++j)
-                    H[i * (i + 1) / 2 + j] = (H[i * (i + 1) / 2 + j] / scale[i]) / scale[j];
-            const double pivot_floor = 64.0 * (parity ? kDblEps : kFltEps);
-#pragma unroll
-            for (int i = 0; i < P; ++i) {
-#pragma unroll
-                for (int j = 0; j <= i; ++j) {
-                    double v = H[i * (i + 1) / 2 + j];
-#pragma unroll
-                    for (int k = 0; k < j; ++k)
-                        v -= H[i * (i + 1) / 2 + k] * H[j * (j + 1) / 2 + k];
-                    if (!isfinite(v) || (i == j && v <= 0.0))
-                        status = kUSingular;
-                    if (i == j) {
-                        const double d = sqrt(v);
-                        H[i * (i + 1) / 2 + i] = d;
-                        inv[i] = 1.0 / d;
-                    } else {
-                        H[i * (i + 1) / 2 + j] = v * inv[j];
-                    }
-                }
-            }
-            if (status == kAvailable) {
-#pragma unroll
-                for (int i = 0; i < P; ++i)
-                    if (!fixed[i] && H[i * (i + 1) / 2 + i] * H[i * (i + 1) / 2 + i] <= pivot_floor)
-                        status = kUSingular;
-            }
+            inv[i] = rsqrt(d);
         }
     }
-    g.sync(); // every lane has read `cur`; the state block becomes column storage
-    if (status == kAvailable) {
-#pragma unroll
-        for (int column = 0; column < P; ++column) {
-            double b[P];
-#pragma unroll
-            for (int i = 0; i < P; ++i)
-                b[i] = (i == column) ? 1.0 / scale[i] : 0.0;
-#pragma unroll
-            for (int i = 0; i < P; ++i) {
-                double v = b[i];
-#pragma unroll
-                for (int j = 0; j < i; ++j)
-                    v -= H[i * (i + 1) / 2 + j] * b[j];
-                b[i] = v * inv[i];
-            }
-#pragma unroll
-            for (int i = P - 1; i >= 0; --i) {
-                double v = b[i];
-#pragma unroll
-                for (int j = i + 1; j < P; ++j)
-                    v -= H[j * (j + 1) / 2 + i] * b[j];
-                b[i] = v * inv[i];
-            }
-#pragma unroll
-            for (int i = 0; i < P; ++i) {
-                const double c = fixed[column] || fixed[i] ? 0.0 : (b[i] / scale[i]) * variance;
-                if (!isfinite(c))
-                    status = kUInvalid;
-                if (int(g.lane) == (i * P + column) % G)
-                    state[i * P + column] = c;
-            }
-        }
-    }
-    g.sync();
-    bool negative = false;
     if (status == kAvailable) {
 #pragma unroll
         for (int i = 0; i < P; ++i)
-            negative = negative || state[i * P + i] < 0.0;
-        if (negative)
-            status = kUInvalid;
+#pragma unroll
+            for (int j = 0; j <= i; ++j)
+                H[i * (i + 1) / 2 + j] = H[i * (i + 1) / 2 + j] * inv[i] * inv[j];
+        const double pivot_floor = 64.0 * (a.policy == kPolicyParity ? kDblEps : kFltEps);
+        double linv[P];
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+#pragma unroll
+            for (int j = 0; j <= i; ++j) {
+                double v = H[i * (i + 1) / 2 + j];
+#pragma unroll
+                for (int k = 0; k < j; ++k)
+                    v -= H[i * (i + 1) / 2 + k] * H[j * (j + 1) / 2 + k];
+                if (!isfinite(v) || (i == j && v <= 0.0))
+                    status = kUSingular;
+                if (i == j) {
+                    linv[i] = rsqrt(v);
+                    H[i * (i + 1) / 2 + i] = v * linv[i];
+                } else {
+                    H[i * (i + 1) / 2 + j] = v * linv[j];
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < P; ++i)
+            if (!fixed[i] && H[i * (i + 1) / 2 + i] * H[i * (i + 1) / 2 + i] <= pivot_floor)
+                status = kUSingular;
+        if (status == kAvailable) {
+            // Column `column` of the inverse into info[.. * P + column].
+#pragma unroll
+            for (int column = 0; column < P; ++column) {
+                double b[P];
+#pragma unroll
+                for (int i = 0; i < P; ++i)
+                    b[i] = (i == column) ? inv[i] : 0.0;
+#pragma unroll
+                for (int i = 0; i < P; ++i) {
+                    double v = b[i];
+#pragma unroll
+                    for (int j = 0; j < i; ++j)
+                        v -= H[i * (i + 1) / 2 + j] * b[j];
+                    b[i] = v * linv[i];
+                }
+#pragma unroll
+                for (int i = P - 1; i >= 0; --i) {
+                    double v = b[i];
+#pragma unroll
+                    for (int j = i + 1; j < P; ++j)
+                        v -= H[j * (j + 1) / 2 + i] * b[j];
+                    b[i] = v * linv[i];
+                }
+#pragma unroll
+                for (int i = 0; i < P; ++i) {
+                    const double c = fixed[column] || fixed[i] ? 0.0 : (b[i] * inv[i]) * variance;
+                    if (!isfinite(c))
+                        status = kUInvalid;
+                    info[i * P + column] = float(c);
+                }
+            }
+        }
     }
-    const float qnan = __int_as_float(0x7fffffff);
-    for (int k = int(g.lane); k < P * P; k += G) {
-        const int i = k / P, j = k % P;
-        const float v = status == kAvailable ? float(state[i * P + j] / 2.0 + state[j * P + i] / 2.0) : qnan;
-        cov_out[k] = i == j && status == kAvailable ? float(state[k]) : v;
+    // Symmetrise (uncertainty.hpp:96-103) or publish NaN on any failure.
+    if (status == kAvailable) {
+#pragma unroll
+        for (int i = 0; i < P; ++i)
+            if (info[i * P + i] < 0.0f)
+                status = kUInvalid;
     }
-    for (int k = int(g.lane); k < P; k += G)
-        se_out[k] = status == kAvailable ? float(sqrt(state[k * P + k])) : qnan;
-    g.sync();
+    if (status == kAvailable) {
+#pragma unroll
+        for (int i = 0; i < P; ++i)
+#pragma unroll
+            for (int j = 0; j < i; ++j) {
+                const float v = info[i * P + j] / 2.0f + info[j * P + i] / 2.0f;
+                info[i * P + j] = v;
+                info[j * P + i] = v;
+            }
+#pragma unroll
+        for (int i = 0; i < P; ++i)
+            se_out[i] = sqrtf(info[i * P + i]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < P * P; ++k)
+            info[k] = qnan;
+#pragma unroll
+        for (int i = 0; i < P; ++i)
+            se_out[i] = qnan;
+    }
     return status;
 }
 
