@@ -211,7 +211,7 @@ int launch_batch(bf_cuda_context *ctx, const bf_fit_args &in, const bf::FitArgs 
     cudaEvent_t k0 = take_event(ctx), k1 = take_event(ctx);
     BF_CUDA(cudaEventRecord(k0, st));
     if (!p0 || guess_only) {
-        BF_CUDA(bf::launch_guess(in.model, lanes, x, y, count, int(in.m), guess_buf, guess_status, ctx->sms, st));
+        BF_CUDA(bf::launch_guess(in.model, x, y, count, int(in.m), guess_buf, guess_status, ctx->sms, st));
         ++ctx->launches;
         p0 = guess_buf;
     }

@@ -29,6 +29,9 @@ template <int G> struct Group {
     template <class T> __device__ __forceinline__ T xor_(T v, int o) const {
         return __shfl_xor_sync(mask, v, o, G);
     }
+    // Value of the previous / next group lane (a lane's own value at the ends).
+    template <class T> __device__ __forceinline__ T prev(T v) const { return __shfl_up_sync(mask, v, 1, G); }
+    template <class T> __device__ __forceinline__ T next(T v) const { return __shfl_down_sync(mask, v, 1, G); }
     // Bit i set <=> pred true on group lane i.
     __device__ __forceinline__ unsigned ballot(bool p) const {
         return (__ballot_sync(mask, p) & mask) >> base;

@@ -67,6 +67,76 @@ template <int G> __device__ __forceinline__ void bitonic_merge(const Group<G> &g
     }
 }
 
+// ------------------------------------------------- sorting in registers --
+// N = G*V values in a blocked layout: group lane l holds elements [l*V, l*V+V).
+// Compare-exchanges across lanes use shuffles, within a lane plain min/max; the
+// network is fully unrolled (k, j are compile-time after unrolling).
+__device__ __forceinline__ void cmpx(float &lo, float &hi, bool ascending) {
+    const float a = lo, b = hi;
+    lo = ascending ? fminf(a, b) : fmaxf(a, b);
+    hi = ascending ? fmaxf(a, b) : fminf(a, b);
+}
+
+template <int G, int V>
+__device__ __forceinline__ void reg_stage(const Group<G> &g, float (&v)[V], int k, int j, bool merge_only) {
+    if (j >= V) {
+        const int lx = j / V;
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const int e = int(g.lane) * V + i;
+            const bool ascending = merge_only || (e & k) == 0;
+            const bool keep_min = ascending == ((e & j) == 0);
+            const float o = g.xor_(v[i], lx);
+            v[i] = keep_min ? fminf(v[i], o) : fmaxf(v[i], o);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            if ((i & j) == 0) {
+                const int e = int(g.lane) * V + i;
+                cmpx(v[i], v[i | j], merge_only || (e & k) == 0);
+            }
+        }
+    }
+}
+
+// Ascending bitonic sort of G*V values.
+template <int G, int V> __device__ __forceinline__ void reg_sort(const Group<G> &g, float (&v)[V]) {
+    constexpr int N = G * V;
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+            reg_stage<G, V>(g, v, k, j, false);
+}
+
+// Ascending sort of a bitonic sequence of G*V values (log2 N stages).
+template <int G, int V> __device__ __forceinline__ void reg_merge(const Group<G> &g, float (&v)[V]) {
+    constexpr int N = G * V;
+#pragma unroll
+    for (int j = N >> 1; j > 0; j >>= 1)
+        reg_stage<G, V>(g, v, N, j, true);
+}
+
+// k-th smallest (0-based) of the union of sorted a[0..na) and b[0..nb): a
+// merge-path binary search for how many of the k+1 smallest come from a.
+__device__ __forceinline__ float kth_of_two(const float *a, int na, const float *b, int nb, int k) {
+    int lo = k + 1 - nb > 0 ? k + 1 - nb : 0;
+    int hi = k + 1 < na ? k + 1 : na;
+    while (lo < hi) {
+        const int i = (lo + hi) >> 1;
+        const int j = k + 1 - i;
+        if (a[i] < b[j - 1])
+            lo = i + 1;
+        else
+            hi = i;
+    }
+    const int j = k + 1 - lo;
+    const float va = lo > 0 ? a[lo - 1] : -__int_as_float(0x7f800000);
+    const float vb = j > 0 ? b[j - 1] : -__int_as_float(0x7f800000);
+    return fmaxf(va, vb);
+}
+
 // detail::median on sorted values (initial_guess.hpp:25-30).
 __device__ __forceinline__ float sorted_median(const float *a, int n) {
     return (n & 1) ? a[n / 2] : midpoint_rn(a[n / 2 - 1], a[n / 2]);
@@ -87,6 +157,9 @@ template <int MODEL> struct Signal {
     __device__ __forceinline__ float smooth(int j) const {
         if (j == 0 || j + 1 == m)
             return at(j);
+        return smooth_interior(j);
+    }
+    __device__ __forceinline__ float smooth_interior(int j) const {
         return radd(radd(rmul(0.25f, at(j - 1)), rmul(0.5f, at(j))), rmul(0.25f, at(j + 1)));
     }
     // detail::raw_maximum (initial_guess.hpp:111-115): first max of s[j-1..j+1].
@@ -103,6 +176,31 @@ template <int MODEL> struct Signal {
         return best;
     }
 };
+
+// Visit every interior sample j (1 <= j <= m-2) in order, G at a time, with its
+// smoothed value and both smoothed neighbours: each smoothed sample is computed
+// once and its neighbours come from the adjacent lanes (the first lane's left
+// neighbour is carried from the previous chunk; the last lane computes its right
+// neighbour).  f(j, value, left, right) runs on lanes with an interior j.
+template <int MODEL, int G, class F>
+__device__ __forceinline__ void scan_smoothed(const Group<G> &g, const Signal<MODEL> &s, F &&f) {
+    const int m = s.m;
+    float carry = s.at(0); // smooth(0) is the raw edge sample
+    for (int t0 = 1; t0 + 1 < m; t0 += G) {
+        const int j = t0 + int(g.lane);
+        const bool inside = j + 1 < m;
+        const float v = inside ? s.smooth_interior(j) : 0.0f;
+        float left = g.prev(v);
+        if (g.lane == 0)
+            left = carry;
+        float right = g.next(v);
+        if (inside && (g.lane == G - 1 || j + 2 >= m))
+            right = s.smooth(j + 1);
+        carry = g.bcast(v, G - 1);
+        if (inside)
+            f(j, v, left, right);
+    }
+}
 
 // Group argmax of (value, index): larger value wins, ties go to the smaller index.
 template <int G> __device__ __forceinline__ void argmax_pair(const Group<G> &g, float &v, int &i) {
@@ -234,7 +332,10 @@ __device__ float prominence(const Group<G> &g, const Signal<MODEL> &s, int index
 // initial_guess<float,Model> for the spectrum ys[0..m).  `scratch` holds 2*n1 floats.
 // Returns the GuessStatus; out[] receives the guessed parameters (NaN when the
 // reference leaves them unset).
-template <int MODEL, int G>
+// V > 0: edge medians sorted in registers, G*V >= max(1, M/10) values per side;
+// V == 0: the general shared-memory path (any M).  `scratch` holds
+// 2*max(n1, G*V) floats.
+template <int MODEL, int G, int V>
 __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *xs, const float *ys,
                              bool y_finite, float *scratch, float *out) {
     constexpr int P = Model<MODEL>::P;
@@ -246,29 +347,90 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
     if (!xc.guess_ok || !y_finite)
         return kGuessInvalid;
     const int m = xc.m, count = xc.count, n1 = xc.n1;
-    // Edge medians (initial_guess.hpp:142-150).
-    const int n1_mask = n1 - 1;
-    for (int t = int(g.lane); t < 2 * n1; t += G) {
-        const int j = t & n1_mask;
-        scratch[t] = j < count ? ys[t >= n1 ? m - count + j : j] : __int_as_float(0x7f800000);
+    float left_level, right_level, baseline, slope, level, noise_median;
+    if constexpr (V > 0) {
+        // Edge medians (initial_guess.hpp:142-150): both sides sorted in registers;
+        // the union median by a merge-path search over the two sorted runs.
+        constexpr int N = G * V;
+        float lv[V], rv[V];
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const int e = int(g.lane) * V + i;
+            lv[i] = e < count ? ys[e] : __int_as_float(0x7f800000);
+            rv[i] = e < count ? ys[m - count + e] : __int_as_float(0x7f800000);
+        }
+        reg_sort<G, V>(g, lv);
+        reg_sort<G, V>(g, rv);
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            scratch[int(g.lane) * V + i] = lv[i];
+            scratch[N + int(g.lane) * V + i] = rv[i];
+        }
+        g.sync();
+        left_level = sorted_median(scratch, count);
+        right_level = sorted_median(scratch + N, count);
+        baseline = midpoint_rn(kth_of_two(scratch, count, scratch + N, count, count - 1),
+                               kth_of_two(scratch, count, scratch + N, count, count));
+        slope = paired ? rdiv(rsub(right_level, left_level), rsub(xc.right_x, xc.left_x)) : 0.0f;
+        level = paired ? left_level : baseline;
+        g.sync();
+        // Absolute deviations of a sorted run from its median fall then rise: a
+        // bitonic sequence, so a bitonic merge sorts each side.
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const int e = int(g.lane) * V + i;
+            lv[i] = e < count ? fabsf(rsub(lv[i], left_level)) : __int_as_float(0x7f800000);
+            rv[i] = e < count ? fabsf(rsub(rv[i], right_level)) : __int_as_float(0x7f800000);
+        }
+        reg_merge<G, V>(g, lv);
+        reg_merge<G, V>(g, rv);
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            scratch[int(g.lane) * V + i] = lv[i];
+            scratch[N + int(g.lane) * V + i] = rv[i];
+        }
+        g.sync();
+        noise_median = midpoint_rn(kth_of_two(scratch, count, scratch + N, count, count - 1),
+                                   kth_of_two(scratch, count, scratch + N, count, count));
+        g.sync();
+    } else {
+        // Edge medians (initial_guess.hpp:142-150) with shared-memory sorts.
+        const int n1_mask = n1 - 1;
+        for (int t = int(g.lane); t < 2 * n1; t += G) {
+            const int j = t & n1_mask;
+            scratch[t] = j < count ? ys[t >= n1 ? m - count + j : j] : __int_as_float(0x7f800000);
+        }
+        g.sync();
+        bitonic_sort(g, scratch, n1, 2);
+        left_level = sorted_median(scratch, count);
+        right_level = sorted_median(scratch + n1, count);
+        g.sync();
+        // Union of both sorted sides: reverse the right run to make one bitonic sequence.
+        for (int t = int(g.lane); t < n1 / 2; t += G) {
+            const float a = scratch[n1 + t], b = scratch[2 * n1 - 1 - t];
+            scratch[n1 + t] = b;
+            scratch[2 * n1 - 1 - t] = a;
+        }
+        g.sync();
+        bitonic_merge(g, scratch, 2 * n1);
+        baseline = sorted_median(scratch, 2 * count);
+        g.sync();
+        slope = paired ? rdiv(rsub(right_level, left_level), rsub(xc.right_x, xc.left_x)) : 0.0f;
+        level = paired ? left_level : baseline;
+        // Absolute edge deviations (initial_guess.hpp:163-167), both sides sorted together.
+        for (int t = int(g.lane); t < 2 * n1; t += G) {
+            float v = __int_as_float(0x7f800000);
+            if (t < count)
+                v = fabsf(rsub(ys[t], left_level));
+            else if (t >= n1 && t - n1 < count)
+                v = fabsf(rsub(ys[m - count + (t - n1)], right_level));
+            scratch[t] = v;
+        }
+        g.sync();
+        bitonic_sort(g, scratch, 2 * n1, 1);
+        noise_median = sorted_median(scratch, 2 * count);
+        g.sync();
     }
-    g.sync();
-    bitonic_sort(g, scratch, n1, 2);
-    const float left_level = sorted_median(scratch, count);
-    const float right_level = sorted_median(scratch + n1, count);
-    g.sync();
-    // Union of both sorted sides: reverse the right run to make one bitonic sequence.
-    for (int t = int(g.lane); t < n1 / 2; t += G) {
-        const float a = scratch[n1 + t], b = scratch[2 * n1 - 1 - t];
-        scratch[n1 + t] = b;
-        scratch[2 * n1 - 1 - t] = a;
-    }
-    g.sync();
-    bitonic_merge(g, scratch, 2 * n1);
-    const float baseline = sorted_median(scratch, 2 * count);
-    g.sync();
-    const float slope = paired ? rdiv(rsub(right_level, left_level), rsub(xc.right_x, xc.left_x)) : 0.0f;
-    const float level = paired ? left_level : baseline;
     if (!isfinite(slope))
         return kGuessInvalid;
     const Signal<MODEL> s{xs, ys, level, slope, xc.left_x, m};
@@ -280,31 +442,18 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
             return kGuessInvalid;
     }
     // Noise scale: 1.4826 * median of absolute edge deviations (initial_guess.hpp:163-169).
-    for (int t = int(g.lane); t < 2 * n1; t += G) {
-        float v = __int_as_float(0x7f800000);
-        if (t < count)
-            v = fabsf(rsub(ys[t], left_level));
-        else if (t >= n1 && t - n1 < count)
-            v = fabsf(rsub(ys[m - count + (t - n1)], right_level));
-        scratch[t] = v;
-    }
-    g.sync();
-    // Pack the right deviations next to the left ones, then sort all 2*n1.
-    bitonic_sort(g, scratch, 2 * n1, 1);
-    const float noise = rmul(1.4826f, sorted_median(scratch, 2 * count));
-    g.sync();
+    const float noise = rmul(1.4826f, noise_median);
     if (!isfinite(noise))
         return kGuessInvalid;
     // Tallest smoothed local maximum (initial_guess.hpp:170-179).
     float height = 0.0f;
     int first = m;
-    for (int j = 1 + int(g.lane); j + 1 < m; j += G) {
-        const float v = s.smooth(j);
-        if (v > 0.0f && v > s.smooth(j - 1) && v >= s.smooth(j + 1) && v > height) {
+    scan_smoothed<MODEL, G>(g, s, [&](int j, float v, float left, float right) {
+        if (v > 0.0f && v > left && v >= right && v > height) {
             height = v;
             first = j;
         }
-    }
+    });
     argmax_pair(g, height, first);
     if (first == m || height <= rmul(3.0f, noise))
         return kGuessNoPeak;
@@ -336,21 +485,20 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         while (true) {
             float bv = 0.0f;
             int bj = m;
-            for (int j = 1 + int(g.lane); j + 1 < m; j += G) {
-                const float v = s.smooth(j);
-                if (!(v > 0.0f && v > s.smooth(j - 1) && v >= s.smooth(j + 1)))
-                    continue;
+            scan_smoothed<MODEL, G>(g, s, [&](int j, float v, float left, float right) {
+                if (!(v > 0.0f && v > left && v >= right))
+                    return;
                 if (!(v < bound_v || (v == bound_v && j > bound_j)))
-                    continue;
+                    return;
                 if (!(v > bv || (v == bv && j < bj)))
-                    continue;
+                    return;
                 const int idx = s.raw_maximum(j);
                 const int bins = idx > first ? idx - first : first - idx;
                 if (bins < 3 || fabsf(rsub(xs[idx], primary.center)) < separation)
-                    continue;
+                    return;
                 bv = v;
                 bj = j;
-            }
+            });
             argmax_pair(g, bv, bj);
             if (bj == m)
                 break;

@@ -37,13 +37,17 @@ __host__ __device__ inline int bank_staggered(int words, int lanes) { return rou
 template <int MODEL> __host__ __device__ inline int lm_group_words(int m, int lanes) {
     return bank_staggered(round_up(m, 4) + 4 * Layout<MODEL>::K, lanes); // y row + 2 FP64 state slots
 }
-__host__ __device__ inline int guess_group_words(int m, int lanes) {
-    return bank_staggered(round_up(m, 4) + 2 * pow2_at_least(edge_count(m)), lanes); // y row + sort scratch
+__host__ __device__ inline int guess_group_words(int m, int lanes, int v) {
+    const int n1 = pow2_at_least(edge_count(m));
+    const int sorted = n1 > lanes * v ? n1 : lanes * v;
+    return bank_staggered(round_up(m, 4) + 2 * sorted, lanes); // y row + sorted edge runs
 }
 __host__ __device__ inline int x_words(int m) { return round_up(m, 4); }
 
 template <int MODEL, int G> int lm_smem_bytes(int m) { return 4 * (x_words(m) + (kBlock / G) * lm_group_words<MODEL>(m, G)); }
-template <int G> int guess_smem_bytes(int m) { return 4 * (x_words(m) + (kBlock / G) * guess_group_words(m, G)); }
+template <int G, int V> int guess_smem_bytes(int m) {
+    return 4 * (x_words(m) + (kBlock / G) * guess_group_words(m, G, V));
+}
 
 // CTA prologue: stage x and derive the grid constants (solver.hpp:58-69,223-239;
 // initial_guess.hpp:131-153).  Called by every thread of the block.
@@ -131,7 +135,9 @@ __device__ __forceinline__ void stage_row(const Group<G> &g, const float *row, i
 }
 
 // ------------------------------------------------------------ guess kernel --
-template <int MODEL, int G>
+// G lanes per spectrum; V edge values per lane sorted in registers (V == 0: the
+// shared-memory sorting path for very long spectra).
+template <int MODEL, int G, int V>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) guess_kernel(const float *x, const float *y, long long n,
                                                                    int m, float *guesses, int32_t *guess_status) {
     constexpr int P = Model<MODEL>::P;
@@ -143,7 +149,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) guess_kernel(const float *
     const XConst cx = xc;
     const Group<G> g;
     const int gid = threadIdx.x / G;
-    float *ys = smem + x_words(m) + gid * guess_group_words(m, G);
+    float *ys = smem + x_words(m) + gid * guess_group_words(m, G, V);
     float *scratch = ys + round_up(m, 4);
     const bool vec_ok = (m & 3) == 0 && (reinterpret_cast<uintptr_t>(y) & 15) == 0;
     for (long long fit = (long long)blockIdx.x * kGroups + gid; fit < n; fit += (long long)gridDim.x * kGroups) {
@@ -151,7 +157,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) guess_kernel(const float *
         float syy;
         stage_row(g, y + fit * (long long)m, m, vec_ok, ys, yfin, flat, syy);
         float p[P];
-        const int gs = initial_guess<MODEL, G>(g, cx, xs, ys, yfin, scratch, p);
+        const int gs = initial_guess<MODEL, G, V>(g, cx, xs, ys, yfin, scratch, p);
 #pragma unroll
         for (int k = 0; k < P; ++k)
             if (int(g.lane) == k)
@@ -437,16 +443,32 @@ static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t strea
     return cudaGetLastError();
 }
 
-template <int MODEL, int G>
+template <int MODEL, int G, int V>
 static cudaError_t launch_guess_typed(const float *x, const float *y, long long n, int m, float *guesses,
                                       int32_t *status, int sms, cudaStream_t stream) {
-    const int smem = guess_smem_bytes<G>(m);
+    const int smem = guess_smem_bytes<G, V>(m);
     int grid = 0, per_sm = 0;
-    cudaError_t e = grid_for(guess_kernel<MODEL, G>, smem, n, kBlock / G, sms, grid, per_sm);
+    cudaError_t e = grid_for(guess_kernel<MODEL, G, V>, smem, n, kBlock / G, sms, grid, per_sm);
     if (e != cudaSuccess)
         return e;
-    guess_kernel<MODEL, G><<<grid, kBlock, smem, stream>>>(x, y, n, m, guesses, status);
+    guess_kernel<MODEL, G, V><<<grid, kBlock, smem, stream>>>(x, y, n, m, guesses, status);
     return cudaGetLastError();
+}
+
+// Group width and register-sort width of the guess for spectra of M points: the
+// edge runs hold max(1, M/10) values each.
+struct GuessShape {
+    int lanes, v;
+};
+__host__ __device__ inline GuessShape guess_shape(int m) {
+    const int n1 = pow2_at_least(edge_count(m));
+    if (n1 <= 128)
+        return {8, n1 / 8 > 1 ? n1 / 8 : 1};
+    if (n1 <= 256)
+        return {16, 16};
+    if (n1 <= 512)
+        return {32, 16};
+    return {32, 0};
 }
 
 template <int MODEL>
@@ -459,12 +481,18 @@ static cudaError_t launch_lm_model(const FitArgs &a, int lanes, int sms, cudaStr
 }
 
 template <int MODEL>
-static cudaError_t launch_guess_model(int lanes, const float *x, const float *y, long long n, int m, float *guesses,
+static cudaError_t launch_guess_model(const float *x, const float *y, long long n, int m, float *guesses,
                                       int32_t *status, int sms, cudaStream_t s) {
-    switch (lanes) {
-    case 8: return launch_guess_typed<MODEL, 8>(x, y, n, m, guesses, status, sms, s);
-    case 16: return launch_guess_typed<MODEL, 16>(x, y, n, m, guesses, status, sms, s);
-    default: return launch_guess_typed<MODEL, 32>(x, y, n, m, guesses, status, sms, s);
+    const GuessShape gs = guess_shape(m);
+    switch (gs.lanes * 100 + gs.v) {
+    case 801: return launch_guess_typed<MODEL, 8, 1>(x, y, n, m, guesses, status, sms, s);
+    case 802: return launch_guess_typed<MODEL, 8, 2>(x, y, n, m, guesses, status, sms, s);
+    case 804: return launch_guess_typed<MODEL, 8, 4>(x, y, n, m, guesses, status, sms, s);
+    case 808: return launch_guess_typed<MODEL, 8, 8>(x, y, n, m, guesses, status, sms, s);
+    case 816: return launch_guess_typed<MODEL, 8, 16>(x, y, n, m, guesses, status, sms, s);
+    case 1616: return launch_guess_typed<MODEL, 16, 16>(x, y, n, m, guesses, status, sms, s);
+    case 3216: return launch_guess_typed<MODEL, 32, 16>(x, y, n, m, guesses, status, sms, s);
+    default: return launch_guess_typed<MODEL, 32, 0>(x, y, n, m, guesses, status, sms, s);
     }
 }
 
@@ -478,13 +506,13 @@ cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStre
     }
 }
 
-cudaError_t launch_guess(int model, int lanes, const float *x, const float *y, long long n, int m, float *guesses,
+cudaError_t launch_guess(int model, const float *x, const float *y, long long n, int m, float *guesses,
                          int32_t *status, int sms, cudaStream_t s) {
     switch (model) {
-    case kGaussian: return launch_guess_model<kGaussian>(lanes, x, y, n, m, guesses, status, sms, s);
-    case kLorentzian: return launch_guess_model<kLorentzian>(lanes, x, y, n, m, guesses, status, sms, s);
-    case kPseudoVoigt: return launch_guess_model<kPseudoVoigt>(lanes, x, y, n, m, guesses, status, sms, s);
-    case kTwoLorentzian: return launch_guess_model<kTwoLorentzian>(lanes, x, y, n, m, guesses, status, sms, s);
+    case kGaussian: return launch_guess_model<kGaussian>(x, y, n, m, guesses, status, sms, s);
+    case kLorentzian: return launch_guess_model<kLorentzian>(x, y, n, m, guesses, status, sms, s);
+    case kPseudoVoigt: return launch_guess_model<kPseudoVoigt>(x, y, n, m, guesses, status, sms, s);
+    case kTwoLorentzian: return launch_guess_model<kTwoLorentzian>(x, y, n, m, guesses, status, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -505,10 +533,11 @@ int smem_bytes(int model, int lanes, int m) {
     case 316: lm = lm_smem_bytes<3, 16>(m); break;
     default: lm = lm_smem_bytes<3, 32>(m); break;
     }
-    switch (lanes) {
-    case 8: gs = guess_smem_bytes<8>(m); break;
-    case 16: gs = guess_smem_bytes<16>(m); break;
-    default: gs = guess_smem_bytes<32>(m); break;
+    const GuessShape shape = guess_shape(m);
+    switch (shape.lanes) {
+    case 8: gs = guess_smem_bytes<8, 16>(m); break;
+    case 16: gs = guess_smem_bytes<16, 16>(m); break;
+    default: gs = shape.v ? guess_smem_bytes<32, 16>(m) : guess_smem_bytes<32, 0>(m); break;
     }
     return lm > gs ? lm : gs;
 }

@@ -12,7 +12,8 @@ namespace bf {
 cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStream_t stream, LaunchInfo *info);
 
 // Launch the data-only guess kernel: guesses[N*P] and, when non-null, status[N].
-cudaError_t launch_guess(int model, int lanes, const float *x, const float *y, long long n, int m, float *guesses,
+// Its group width follows from M.
+cudaError_t launch_guess(int model, const float *x, const float *y, long long n, int m, float *guesses,
                          int32_t *status, int sms, cudaStream_t stream);
 
 // Dynamic shared memory of one CTA for (model, lanes, M).

@@ -102,7 +102,7 @@ int bf_cuda_fit_noalloc(const bf_fit_args *args, const bf_fit_outputs *out, void
     float *guesses = reinterpret_cast<float *>(scratch + kCounterBytes);
     const float *p0 = args->p0;
     if (!p0) {
-        e = bf::launch_guess(args->model, lanes, args->x, args->y, (long long)args->n, int(args->m), guesses,
+        e = bf::launch_guess(args->model, args->x, args->y, (long long)args->n, int(args->m), guesses,
                              nullptr, sms, st);
         if (e != cudaSuccess)
             return bf::host::report_cuda(e, "guess kernel");
