@@ -181,25 +181,43 @@ template <int MODEL> struct Signal {
 // smoothed value and both smoothed neighbours: each smoothed sample is computed
 // once and its neighbours come from the adjacent lanes (the first lane's left
 // neighbour is carried from the previous chunk; the last lane computes its right
-// neighbour).  f(j, value, left, right) runs on lanes with an interior j.
+// neighbour).  Two chunks are in flight per step.  f(j, value, left, right) runs on
+// lanes with an interior j.  Returns whether every signal sample is finite.
 template <int MODEL, int G, class F>
-__device__ __forceinline__ void scan_smoothed(const Group<G> &g, const Signal<MODEL> &s, F &&f) {
+__device__ __forceinline__ bool scan_smoothed(const Group<G> &g, const Signal<MODEL> &s, F &&f) {
     const int m = s.m;
-    float carry = s.at(0); // smooth(0) is the raw edge sample
-    for (int t0 = 1; t0 + 1 < m; t0 += G) {
-        const int j = t0 + int(g.lane);
-        const bool inside = j + 1 < m;
-        const float v = inside ? s.smooth_interior(j) : 0.0f;
-        float left = g.prev(v);
-        if (g.lane == 0)
-            left = carry;
-        float right = g.next(v);
-        if (inside && (g.lane == G - 1 || j + 2 >= m))
-            right = s.smooth(j + 1);
-        carry = g.bcast(v, G - 1);
-        if (inside)
-            f(j, v, left, right);
+    const float first = s.at(0);
+    float carry = first; // smooth(0) is the raw edge sample
+    bool finite = isfinite(first) & isfinite(s.at(m - 1));
+    for (int t0 = 1; t0 + 1 < m; t0 += 2 * G) {
+        const int j0 = t0 + int(g.lane), j1 = j0 + G;
+        const bool in0 = j0 + 1 < m, in1 = j1 + 1 < m;
+        const float s0 = in0 ? s.at(j0) : 0.0f, s1 = in1 ? s.at(j1) : 0.0f;
+        finite = finite & isfinite(s0) & isfinite(s1);
+        const float v0 = in0 ? radd(radd(rmul(0.25f, s.at(j0 - 1)), rmul(0.5f, s0)), rmul(0.25f, s.at(j0 + 1)))
+                             : 0.0f;
+        const float v1 = in1 ? radd(radd(rmul(0.25f, s.at(j1 - 1)), rmul(0.5f, s1)), rmul(0.25f, s.at(j1 + 1)))
+                             : 0.0f;
+        float l0 = g.prev(v0), l1 = g.prev(v1);
+        float r0 = g.next(v0), r1 = g.next(v1);
+        const float last0 = g.bcast(v0, G - 1), first1 = g.bcast(v1, 0), last1 = g.bcast(v1, G - 1);
+        if (g.lane == 0) {
+            l0 = carry;
+            l1 = last0;
+        }
+        if (g.lane == G - 1)
+            r0 = first1;
+        if (in0 && j0 + 2 >= m)
+            r0 = s.smooth(j0 + 1);
+        if (in1 && (g.lane == G - 1 || j1 + 2 >= m))
+            r1 = s.smooth(j1 + 1);
+        carry = last1;
+        if (in0)
+            f(j0, v0, l0, r0);
+        if (in1)
+            f(j1, v1, l1, r1);
     }
+    return finite;
 }
 
 // Group argmax of (value, index): larger value wins, ties go to the smaller index.
@@ -434,26 +452,23 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
     if (!isfinite(slope))
         return kGuessInvalid;
     const Signal<MODEL> s{xs, ys, level, slope, xc.left_x, m};
-    {
-        bool finite = true;
-        for (int j = int(g.lane); j < m; j += G)
-            finite = finite && isfinite(s.at(j));
-        if (!g.all(finite))
-            return kGuessInvalid;
-    }
     // Noise scale: 1.4826 * median of absolute edge deviations (initial_guess.hpp:163-169).
     const float noise = rmul(1.4826f, noise_median);
     if (!isfinite(noise))
         return kGuessInvalid;
-    // Tallest smoothed local maximum (initial_guess.hpp:170-179).
+    // Tallest smoothed local maximum (initial_guess.hpp:170-179).  The same sweep
+    // checks that every signal sample is finite (initial_guess.hpp:158-162); both
+    // failures end in invalid_input, so their order does not matter.
     float height = 0.0f;
     int first = m;
-    scan_smoothed<MODEL, G>(g, s, [&](int j, float v, float left, float right) {
+    const bool signal_finite = scan_smoothed<MODEL, G>(g, s, [&](int j, float v, float left, float right) {
         if (v > 0.0f && v > left && v >= right && v > height) {
             height = v;
             first = j;
         }
     });
+    if (!g.all(signal_finite))
+        return kGuessInvalid;
     argmax_pair(g, height, first);
     if (first == m || height <= rmul(3.0f, noise))
         return kGuessNoPeak;
