@@ -83,29 +83,22 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
 #pragma unroll
     for (int i = 0; i < TP; ++i)
         aa[i] = 0.0f;
-    for (int base = int(g.lane); base < m; base += G * kChunk) {
-        float part[KC];
+    // Full chunks without per-point bounds checks, then one masked tail chunk.
+    const int full = m - m % (G * kChunk);
+    auto point = [&](int j, float (&part)[KC]) {
+        float J[P];
+        const float r = Model<MODEL>::residual(q, xs[j], ys[j], J);
+        part[0] = fmaf(r, r, part[0]);
 #pragma unroll
-        for (int i = 0; i < KC; ++i)
-            part[i] = 0.0f;
+        for (int k = 0; k < P; ++k) {
+            part[1 + k] = fmaf(J[k], r, part[1 + k]);
 #pragma unroll
-        for (int c = 0; c < kChunk; ++c) {
-            const int j = base + c * G;
-            if (j < m) {
-                float J[P];
-                const float f = Model<MODEL>::eval(q, xs[j], J);
-                const float r = ys[j] - f;
-                part[0] = fmaf(r, r, part[0]);
-#pragma unroll
-                for (int k = 0; k < P; ++k) {
-                    part[1 + k] = fmaf(J[k], r, part[1 + k]);
-#pragma unroll
-                    for (int l = 0; l <= k; ++l)
-                        aa[k * (k + 1) / 2 + l] = fmaf(J[k], J[l], aa[k * (k + 1) / 2 + l]);
-                }
-            }
+            for (int l = 0; l <= k; ++l)
+                aa[k * (k + 1) / 2 + l] = fmaf(J[k], J[l], aa[k * (k + 1) / 2 + l]);
         }
-        // Kahan fold; lo holds minus the Kahan correction, so the value is hi + lo.
+    };
+    // Kahan fold; lo holds minus the Kahan correction, so the value is hi + lo.
+    auto fold = [&](const float (&part)[KC]) {
 #pragma unroll
         for (int i = 0; i < KC; ++i) {
             const float adjusted = __fadd_rn(part[i], lo[i]);
@@ -113,6 +106,29 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
             lo[i] = __fsub_rn(adjusted, __fsub_rn(next, hi[i]));
             hi[i] = next;
         }
+    };
+    for (int base = int(g.lane); base < full; base += G * kChunk) {
+        float part[KC];
+#pragma unroll
+        for (int i = 0; i < KC; ++i)
+            part[i] = 0.0f;
+#pragma unroll
+        for (int c = 0; c < kChunk; ++c)
+            point(base + c * G, part);
+        fold(part);
+    }
+    if (full < m) {
+        float part[KC];
+#pragma unroll
+        for (int i = 0; i < KC; ++i)
+            part[i] = 0.0f;
+#pragma unroll
+        for (int c = 0; c < kChunk; ++c) {
+            const int j = full + int(g.lane) + c * G;
+            if (j < m)
+                point(j, part);
+        }
+        fold(part);
     }
     bool finite = reduce_scatter_store<G, KCP>(g, hi, lo, state, KC);
     finite = reduce_scatter_store_plain<G, TP>(g, aa, state + KC, T) && finite;
@@ -122,26 +138,29 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
 }
 
 // In-place Cholesky of a packed lower triangle (FP64) and solve of rhs.
-// Mirrors detail::cholesky_solve (solver.hpp:98-143), including the optional
-// diagonal equilibration and every finiteness/positivity rejection.
+// Mirrors detail::cholesky_solve (solver.hpp:98-143): the optional diagonal
+// equilibration and every finiteness/positivity rejection.  Pivots use rsqrt
+// (one reciprocal square root instead of a root and a division), and a failure
+// is recorded in a flag instead of an early return, so the groups of a warp do
+// not diverge inside the factorisation; the result is only used when it is true.
 template <int P>
 __device__ __forceinline__ bool chol_solve(double (&a)[P * (P + 1) / 2], double (&b)[P], bool scaled) {
     auto at = [](int i, int j) { return i * (i + 1) / 2 + j; };
-    double scale[P];
+    bool ok = true;
+    double sinv[P];
     if (scaled) {
 #pragma unroll
         for (int i = 0; i < P; ++i) {
             const double d = a[at(i, i)];
-            if (!isfinite(d) || d <= 0.0)
-                return false;
-            scale[i] = sqrt(d);
+            ok = ok & isfinite(d) & (d > 0.0);
+            sinv[i] = rsqrt(d);
         }
 #pragma unroll
         for (int i = 0; i < P; ++i) {
-            b[i] /= scale[i];
+            b[i] *= sinv[i];
 #pragma unroll
             for (int j = 0; j <= i; ++j)
-                a[at(i, j)] = (a[at(i, j)] / scale[i]) / scale[j];
+                a[at(i, j)] = (a[at(i, j)] * sinv[i]) * sinv[j];
         }
     }
     double inv[P];
@@ -153,12 +172,11 @@ __device__ __forceinline__ bool chol_solve(double (&a)[P * (P + 1) / 2], double 
 #pragma unroll
             for (int k = 0; k < j; ++k)
                 v -= a[at(i, k)] * a[at(j, k)];
-            if (!isfinite(v) || (i == j && v <= 0.0))
-                return false;
+            ok = ok & isfinite(v);
             if (i == j) {
-                const double d = sqrt(v);
-                a[at(i, i)] = d;
-                inv[i] = 1.0 / d;
+                ok = ok & (v > 0.0);
+                inv[i] = rsqrt(v);
+                a[at(i, i)] = v * inv[i];
             } else {
                 a[at(i, j)] = v * inv[j];
             }
@@ -176,18 +194,16 @@ __device__ __forceinline__ bool chol_solve(double (&a)[P * (P + 1) / 2], double 
         for (int j = i + 1; j < P; ++j)
             v -= a[at(j, i)] * b[j];
         b[i] = v * inv[i];
-        if (!isfinite(b[i]))
-            return false;
+        ok = ok & isfinite(b[i]);
     }
     if (scaled) {
 #pragma unroll
         for (int i = 0; i < P; ++i) {
-            b[i] /= scale[i];
-            if (!isfinite(b[i]))
-                return false;
+            b[i] *= sinv[i];
+            ok = ok & isfinite(b[i]);
         }
     }
-    return true;
+    return ok;
 }
 
 // free_shape (solver.hpp:70-82).

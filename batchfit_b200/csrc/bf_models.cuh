@@ -30,7 +30,7 @@ template <> struct Model<kGaussian> {
         const float iw = 1.0f / p[2];
         return {p[0], p[1], iw, p[0] * iw};
     }
-    __device__ __forceinline__ static float eval(const Pre &q, float x, float *J) {
+    __device__ __forceinline__ static float residual(const Pre &q, float x, float y, float *J) {
         const float z = (x - q.c) * q.iw;
         // exp(-z^2/2) = 2^(-log2(e)/2 * z^2)
         const float g = ex2_approx(z * z * -0.72134752044448170368f);
@@ -38,7 +38,7 @@ template <> struct Model<kGaussian> {
         J[0] = g;
         J[1] = t;
         J[2] = t * z;
-        return q.a * g;
+        return fmaf(-q.a, g, y);
     }
 };
 
@@ -54,14 +54,14 @@ template <> struct Model<kLorentzian> {
         const float iw = 1.0f / p[2];
         return {p[0], p[1], iw, 2.0f * p[0] * iw};
     }
-    __device__ __forceinline__ static float eval(const Pre &q, float x, float *J) {
+    __device__ __forceinline__ static float residual(const Pre &q, float x, float y, float *J) {
         const float z = (x - q.c) * q.iw;
         const float s = rcp_approx(fmaf(z, z, 1.0f));
         const float t = q.a2iw * s * s * z;
         J[0] = s;
         J[1] = t;
         J[2] = t * z;
-        return q.a * s;
+        return fmaf(-q.a, s, y);
     }
 };
 
@@ -72,25 +72,27 @@ template <> struct Model<kPseudoVoigt> {
     static constexpr bool paired = false;
     static constexpr float width_factor = 1.0f;
     struct Pre {
-        float a, c, iw, eta, a8iw, gln2;
+        float a, c, iw, eta, kl, kg; // kl = 8 a eta / w, kg = 8 a (1-eta) ln2 / w
     };
     __device__ __forceinline__ static Pre prepare(const float *p) {
         const float iw = 1.0f / p[2];
-        return {p[0], p[1], iw, p[3], 8.0f * p[0] * iw, (1.0f - p[3]) * 0.69314718055994530942f};
+        const float a8iw = 8.0f * p[0] * iw;
+        return {p[0], p[1], iw, p[3], a8iw * p[3], a8iw * ((1.0f - p[3]) * 0.69314718055994530942f)};
     }
-    __device__ __forceinline__ static float eval(const Pre &q, float x, float *J) {
+    __device__ __forceinline__ static float residual(const Pre &q, float x, float y, float *J) {
         const float z = (x - q.c) * q.iw;
         const float z2 = z * z;
         const float g = ex2_approx(-4.0f * z2); // exp(-4 ln2 z^2) == 2^(-4 z^2)
         const float l = rcp_approx(fmaf(4.0f, z2, 1.0f));
         const float d = l - g;
         const float s = fmaf(q.eta, d, g); // (1-eta) g + eta l
-        const float t = q.a8iw * fmaf(q.eta * l, l, q.gln2 * g) * z;
+        // df/dc = 8a/w z ((1-eta) ln2 g + eta l^2)
+        const float t = fmaf(q.kl * l, l, q.kg * g) * z;
         J[0] = s;
         J[1] = t;
         J[2] = t * z;
         J[3] = q.a * d;
-        return q.a * s;
+        return fmaf(-q.a, s, y);
     }
 };
 
@@ -106,7 +108,7 @@ template <> struct Model<kTwoLorentzian> {
         const float iw1 = 1.0f / p[2], iw2 = 1.0f / p[5];
         return {p[0], p[1], iw1, 2.0f * p[0] * iw1, p[3], p[4], iw2, 2.0f * p[3] * iw2, p[6], p[7]};
     }
-    __device__ __forceinline__ static float eval(const Pre &q, float x, float *J) {
+    __device__ __forceinline__ static float residual(const Pre &q, float x, float y, float *J) {
         const float z1 = (x - q.c1) * q.iw1;
         const float s1 = rcp_approx(fmaf(z1, z1, 1.0f));
         const float t1 = q.k1 * s1 * s1 * z1;
@@ -121,7 +123,7 @@ template <> struct Model<kTwoLorentzian> {
         J[5] = t2 * z2;
         J[6] = 1.0f;
         J[7] = x;
-        return fmaf(q.a1, s1, fmaf(q.a2, s2, fmaf(q.b1, x, q.b0)));
+        return y - fmaf(q.a1, s1, fmaf(q.a2, s2, fmaf(q.b1, x, q.b0)));
     }
 };
 
