@@ -90,6 +90,10 @@ class Timing(C.Structure):
         ("group_lanes", C.c_int32),
         ("grid", C.c_int32),
         ("blocks_per_sm", C.c_int32),
+        ("guess_ms", C.c_double),
+        ("lm_ms", C.c_double),
+        ("covariance_ms", C.c_double),
+        ("batches", C.c_uint32),
     ]
 
 

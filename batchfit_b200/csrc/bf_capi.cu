@@ -78,6 +78,12 @@ constexpr int kSlots = 2;
 
 } // namespace
 
+// Events around the kernels of one batch: guess = [start, guessed), LM =
+// [guessed, fitted), covariance = [fitted, done).
+struct KernelEvents {
+    cudaEvent_t start, guessed, fitted, done;
+};
+
 struct bf_cuda_context {
     int device = 0;
     int sms = 0;
@@ -88,8 +94,8 @@ struct bf_cuda_context {
     DeviceBuffer x;
     Slot slot[kSlots];
     bf_cuda_timing last{};
-    // Kernel-event pairs of the in-flight submission (one per chunk).
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kernel_events;
+    // Kernel events of the in-flight submission (one set per chunk).
+    std::vector<KernelEvents> kernel_events;
     std::vector<cudaEvent_t> event_pool;
     int launches = 0;
     int lanes = 0;
@@ -208,13 +214,15 @@ cudaEvent_t take_event(bf_cuda_context *ctx) {
 int launch_batch(bf_cuda_context *ctx, const bf_fit_args &in, const bf::FitArgs &base, int lanes, const float *x,
                  const float *y, const float *p0, float *guess_buf, int32_t *guess_status, bool guess_only,
                  const bf_fit_outputs &dev_out, unsigned long long *counter, long long count, cudaStream_t st) {
-    cudaEvent_t k0 = take_event(ctx), k1 = take_event(ctx);
-    BF_CUDA(cudaEventRecord(k0, st));
+    // Four events bracket the guess, LM and covariance kernels of this batch.
+    KernelEvents ev{take_event(ctx), take_event(ctx), take_event(ctx), take_event(ctx)};
+    BF_CUDA(cudaEventRecord(ev.start, st));
     if (!p0 || guess_only) {
         BF_CUDA(bf::launch_guess(in.model, x, y, count, int(in.m), guess_buf, guess_status, ctx->sms, st));
         ++ctx->launches;
         p0 = guess_buf;
     }
+    BF_CUDA(cudaEventRecord(ev.guessed, st));
     if (!guess_only) {
         bf::FitArgs a = base;
         a.x = x;
@@ -230,11 +238,13 @@ int launch_batch(bf_cuda_context *ctx, const bf_fit_args &in, const bf::FitArgs 
         a.n = count;
         a.work_counter = counter;
         BF_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
-        BF_CUDA(bf::launch_fit(in.model, lanes, a, ctx->sms, st, &ctx->info));
+        BF_CUDA(bf::launch_fit(in.model, lanes, a, ctx->sms, st, &ctx->info, ev.fitted));
         ctx->launches += in.uncertainties ? 2 : 1; // LM kernel (+ covariance kernel)
+    } else {
+        BF_CUDA(cudaEventRecord(ev.fitted, st));
     }
-    BF_CUDA(cudaEventRecord(k1, st));
-    ctx->kernel_events.push_back({k0, k1});
+    BF_CUDA(cudaEventRecord(ev.done, st));
+    ctx->kernel_events.push_back(ev);
     return BF_OK;
 }
 
@@ -246,10 +256,9 @@ int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &o
     ctx->lanes = lanes;
     ctx->launches = 0;
     ctx->info = bf::LaunchInfo{};
-    for (auto &ev : ctx->kernel_events) {
-        ctx->event_pool.push_back(ev.first);
-        ctx->event_pool.push_back(ev.second);
-    }
+    for (auto &ev : ctx->kernel_events)
+        for (cudaEvent_t e : {ev.start, ev.guessed, ev.fitted, ev.done})
+            ctx->event_pool.push_back(e);
     ctx->kernel_events.clear();
     BF_CUDA(cudaSetDevice(ctx->device));
     BF_CUDA(cudaEventRecord(ctx->start, ctx->stream[0]));
@@ -355,13 +364,22 @@ int finish(bf_cuda_context *ctx) {
     BF_CUDA(cudaEventSynchronize(ctx->stop));
     float total = 0.0f;
     BF_CUDA(cudaEventElapsedTime(&total, ctx->start, ctx->stop));
-    double kernel = 0.0;
+    double kernel = 0.0, guess = 0.0, lm = 0.0, cov = 0.0;
     for (auto &ev : ctx->kernel_events) {
-        float t = 0.0f;
-        BF_CUDA(cudaEventElapsedTime(&t, ev.first, ev.second));
-        kernel += t;
+        float t[3] = {0.0f, 0.0f, 0.0f};
+        BF_CUDA(cudaEventElapsedTime(&t[0], ev.start, ev.guessed));
+        BF_CUDA(cudaEventElapsedTime(&t[1], ev.guessed, ev.fitted));
+        BF_CUDA(cudaEventElapsedTime(&t[2], ev.fitted, ev.done));
+        guess += t[0];
+        lm += t[1];
+        cov += t[2];
+        kernel += double(t[0]) + t[1] + t[2];
     }
     ctx->last.kernel_ms = kernel;
+    ctx->last.guess_ms = guess;
+    ctx->last.lm_ms = lm;
+    ctx->last.covariance_ms = cov;
+    ctx->last.batches = uint32_t(ctx->kernel_events.size());
     ctx->last.total_ms = total;
     ctx->last.launches = uint32_t(ctx->launches);
     ctx->last.group_lanes = ctx->lanes;
@@ -472,10 +490,9 @@ void bf_cuda_context_destroy(bf_cuda_context *ctx) {
         s.counter.release();
     }
     ctx->x.release();
-    for (auto &ev : ctx->kernel_events) {
-        cudaEventDestroy(ev.first);
-        cudaEventDestroy(ev.second);
-    }
+    for (auto &ev : ctx->kernel_events)
+        for (cudaEvent_t e : {ev.start, ev.guessed, ev.fitted, ev.done})
+            cudaEventDestroy(e);
     for (auto ev : ctx->event_pool)
         cudaEventDestroy(ev);
     for (cudaEvent_t ev : {ctx->start, ctx->stop, ctx->joined})

@@ -427,7 +427,8 @@ template <class K> static cudaError_t grid_for(K kernel, int smem, long long gro
 }
 
 template <int MODEL, int G>
-static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t stream, LaunchInfo *info) {
+static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t stream, LaunchInfo *info,
+                                   cudaEvent_t lm_done) {
     const int smem = lm_smem_bytes<MODEL, G>(a.m);
     int grid = 0, per_sm = 0;
     cudaError_t e = grid_for(lm_kernel<MODEL, G>, smem, a.n, kBlock / G, sms, grid, per_sm);
@@ -437,6 +438,8 @@ static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t strea
     if (info)
         *info = LaunchInfo{grid, kBlock, smem, per_sm, G};
     e = cudaGetLastError();
+    if (e == cudaSuccess && lm_done)
+        e = cudaEventRecord(lm_done, stream);
     if (e != cudaSuccess || !a.uncertainties || a.n == 0)
         return e;
     covariance_kernel<MODEL><<<unsigned((a.n + kCovBlock - 1) / kCovBlock), kCovBlock, 0, stream>>>(a);
@@ -472,11 +475,12 @@ __host__ __device__ inline GuessShape guess_shape(int m) {
 }
 
 template <int MODEL>
-static cudaError_t launch_lm_model(const FitArgs &a, int lanes, int sms, cudaStream_t s, LaunchInfo *info) {
+static cudaError_t launch_lm_model(const FitArgs &a, int lanes, int sms, cudaStream_t s, LaunchInfo *info,
+                                   cudaEvent_t lm_done) {
     switch (lanes) {
-    case 8: return launch_lm_typed<MODEL, 8>(a, sms, s, info);
-    case 16: return launch_lm_typed<MODEL, 16>(a, sms, s, info);
-    default: return launch_lm_typed<MODEL, 32>(a, sms, s, info);
+    case 8: return launch_lm_typed<MODEL, 8>(a, sms, s, info, lm_done);
+    case 16: return launch_lm_typed<MODEL, 16>(a, sms, s, info, lm_done);
+    default: return launch_lm_typed<MODEL, 32>(a, sms, s, info, lm_done);
     }
 }
 
@@ -496,12 +500,13 @@ static cudaError_t launch_guess_model(const float *x, const float *y, long long 
     }
 }
 
-cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStream_t s, LaunchInfo *info) {
+cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStream_t s, LaunchInfo *info,
+                       cudaEvent_t lm_done) {
     switch (model) {
-    case kGaussian: return launch_lm_model<kGaussian>(a, lanes, sms, s, info);
-    case kLorentzian: return launch_lm_model<kLorentzian>(a, lanes, sms, s, info);
-    case kPseudoVoigt: return launch_lm_model<kPseudoVoigt>(a, lanes, sms, s, info);
-    case kTwoLorentzian: return launch_lm_model<kTwoLorentzian>(a, lanes, sms, s, info);
+    case kGaussian: return launch_lm_model<kGaussian>(a, lanes, sms, s, info, lm_done);
+    case kLorentzian: return launch_lm_model<kLorentzian>(a, lanes, sms, s, info, lm_done);
+    case kPseudoVoigt: return launch_lm_model<kPseudoVoigt>(a, lanes, sms, s, info, lm_done);
+    case kTwoLorentzian: return launch_lm_model<kTwoLorentzian>(a, lanes, sms, s, info, lm_done);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -8,8 +8,10 @@ namespace bf {
 // Launch the persistent LM kernel for `model` with `lanes` (8, 16 or 32) lanes per
 // fit on `stream`, followed by the covariance kernel when a.uncertainties.  a.p0
 // must hold initial values for every fit (the user's, or the guess kernel's
-// output).  The caller zeroes a.work_counter (when non-null) first.
-cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStream_t stream, LaunchInfo *info);
+// output).  The caller zeroes a.work_counter (when non-null) first.  When lm_done
+// is non-null it is recorded on `stream` between the two kernels.
+cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStream_t stream, LaunchInfo *info,
+                       cudaEvent_t lm_done = nullptr);
 
 // Launch the data-only guess kernel: guesses[N*P] and, when non-null, status[N].
 // Its group width follows from M.

@@ -106,12 +106,16 @@ typedef struct bf_cuda_pending bf_cuda_pending;
 
 /* Timing of the last completed call on a context (CUDA events, milliseconds). */
 typedef struct bf_cuda_timing {
-    double kernel_ms;   /* fit kernel(s) only */
+    double kernel_ms;   /* fit kernel(s) only: guess + LM + covariance */
     double total_ms;    /* whole call including copies */
     uint32_t launches;  /* fit kernel launches */
     int32_t group_lanes;
     int32_t grid;
     int32_t blocks_per_sm;
+    double guess_ms;      /* data-only guess kernel(s) */
+    double lm_ms;         /* LM kernel(s) */
+    double covariance_ms; /* covariance kernel(s) */
+    uint32_t batches;     /* device batches (chunks) the call ran */
 } bf_cuda_timing;
 
 const char *bf_cuda_last_error(void);
