@@ -28,6 +28,20 @@ struct FitArgs {
     float lower[8], upper[8];
 };
 
+// Values derived from a shared x grid (computed once per CTA, or once per batch
+// segment).
+struct XConst {
+    int m;
+    int x_finite;        // every x finite (solver.hpp:223-226)
+    int varied_x;        // some x differs from x[0] (solver.hpp:238-239)
+    float spacing;       // detail::grid_spacing (solver.hpp:58-69)
+    int guess_ok;        // M>=5, finite, strictly increasing, finite span (initial_guess.hpp:131-141)
+    float guess_spacing; // min x[j]-x[j-1] (initial_guess.hpp:133-139)
+    int count;           // max(1, M/10) edge samples per side (initial_guess.hpp:142)
+    int n1;              // power of two >= count (sorting width per side)
+    float left_x, right_x; // edge-median abscissae (initial_guess.hpp:151-153)
+};
+
 struct LaunchInfo {
     int grid, block, smem, blocks_per_sm, group_lanes;
 };

@@ -103,6 +103,16 @@ __device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
     e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
 }
 
+__host__ __device__ inline int round_up(int v, int a) { return (v + a - 1) / a * a; }
+// Edge samples per side of the data-only guess: max(1, M/10) (initial_guess.hpp:142).
+__host__ __device__ inline int edge_count(int m) { return m / 10 > 1 ? m / 10 : 1; }
+__host__ __device__ inline int pow2_at_least(int v) {
+    int p = 1;
+    while (p < v)
+        p <<= 1;
+    return p;
+}
+
 __host__ __device__ constexpr int pow2ceil(int v) {
     int p = 1;
     while (p < v)

@@ -14,19 +14,6 @@ namespace bf {
 
 enum GuessStatus : int { kGuessSuccess = 0, kGuessInvalid = 1, kGuessNoPeak = 2, kGuessInsufficient = 3 };
 
-// Values derived from the shared x grid, computed once per CTA.
-struct XConst {
-    int m;
-    int x_finite;        // every x finite (solver.hpp:223-226)
-    int varied_x;        // some x differs from x[0] (solver.hpp:238-239)
-    float spacing;       // detail::grid_spacing (solver.hpp:58-69)
-    int guess_ok;        // M>=5, finite, strictly increasing, finite span (initial_guess.hpp:131-141)
-    float guess_spacing; // min x[j]-x[j-1] (initial_guess.hpp:133-139)
-    int count;           // max(1, M/10) edge samples per side (initial_guess.hpp:142)
-    int n1;              // power of two >= count (sorting width per side)
-    float left_x, right_x; // edge-median abscissae (initial_guess.hpp:151-153)
-};
-
 // Ascending bitonic sort of `batches` consecutive arrays of n (power of two) floats.
 // Index arithmetic is shifts and masks only (n is a power of two).
 template <int G>

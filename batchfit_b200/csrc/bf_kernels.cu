@@ -21,15 +21,6 @@ namespace bf {
 constexpr int kBlock = 256;
 constexpr int kMinBlocks = 2;
 
-__host__ __device__ inline int round_up(int v, int a) { return (v + a - 1) / a * a; }
-__host__ __device__ inline int edge_count(int m) { return m / 10 > 1 ? m / 10 : 1; }
-__host__ __device__ inline int pow2_at_least(int v) {
-    int p = 1;
-    while (p < v)
-        p <<= 1;
-    return p;
-}
-
 // Per-group shared memory, in 4-byte words, padded so that consecutive groups of a
 // warp start G banks apart.
 __host__ __device__ inline int bank_staggered(int words, int lanes) { return round_up(words, 32) + (lanes % 32); }
@@ -99,41 +90,6 @@ __device__ void cta_prologue(const float *x, int m, float *xs, XConst &xc) {
     __syncthreads();
 }
 
-// Stage one fit-major y row into shared memory; reports finiteness, flatness
-// (every value equal to y[0]) and sum(y^2).
-template <int G>
-__device__ __forceinline__ void stage_row(const Group<G> &g, const float *row, int m, bool vec_ok, float *ys,
-                                          bool &yfin, bool &flat, float &syy) {
-    const float y0 = __ldg(row);
-    yfin = true;
-    flat = true;
-    syy = 0.0f;
-    if (vec_ok) {
-        const float4 *row4 = reinterpret_cast<const float4 *>(row);
-        for (int v = int(g.lane); v < m / 4; v += G) {
-            const float4 t = __ldcs(row4 + v);
-            reinterpret_cast<float4 *>(ys)[v] = t;
-            yfin = yfin && isfinite(t.x) && isfinite(t.y) && isfinite(t.z) && isfinite(t.w);
-            flat = flat && t.x == y0 && t.y == y0 && t.z == y0 && t.w == y0;
-            syy = fmaf(t.x, t.x, fmaf(t.y, t.y, fmaf(t.z, t.z, fmaf(t.w, t.w, syy))));
-        }
-    } else {
-        for (int j = int(g.lane); j < m; j += G) {
-            const float t = __ldcs(row + j);
-            ys[j] = t;
-            yfin = yfin && isfinite(t);
-            flat = flat && t == y0;
-            syy = fmaf(t, t, syy);
-        }
-    }
-    yfin = g.all(yfin);
-    flat = g.all(flat);
-#pragma unroll
-    for (int o = G / 2; o >= 1; o >>= 1)
-        syy += g.xor_(syy, o);
-    g.sync();
-}
-
 // ------------------------------------------------------------ guess kernel --
 // G lanes per spectrum; V edge values per lane sorted in registers (V == 0: the
 // shared-memory sorting path for very long spectra).
@@ -169,20 +125,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) guess_kernel(const float *
 }
 
 // --------------------------------------------------------------- LM kernel --
-template <int MODEL, int G>
-__device__ __forceinline__ void write_fit(const Group<G> &g, const FitArgs &a, long long fit, const LmState<MODEL> &s) {
-    constexpr int P = Model<MODEL>::P;
-#pragma unroll
-    for (int k = 0; k < P; ++k)
-        if (int(g.lane) == k)
-            a.params[fit * P + k] = s.p[k];
-    if (g.lane == 0) {
-        a.status[fit] = s.status;
-        a.iterations[fit] = s.iterations;
-        a.chi2[fit] = float(s.chi2);
-    }
-}
-
 template <int MODEL, int G>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) lm_kernel(FitArgs a) {
     constexpr int P = Model<MODEL>::P;
@@ -247,15 +189,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) lm_kernel(FitArgs a) {
             done = lm_plan<MODEL>(a, cx, double(syy), state, s);
         if (done) {
             write_fit<MODEL, G>(g, a, fit, s);
-            if (a.uncertainties && s.status == kConverged) {
-                // The accepted J^T J (the information matrix at the reported
-                // parameters) for covariance_kernel, in the covariance output.
-                const double *cur = state + s.cur * Layout<MODEL>::K;
-                for (int k = int(g.lane); k < P * P; k += G) {
-                    const int i = k / P, j = k % P;
-                    a.covariance[fit * P * P + k] = float(cur[Layout<MODEL>::tri(i > j ? i : j, i > j ? j : i)]);
-                }
-            }
+            if (a.uncertainties && s.status == kConverged)
+                write_information<MODEL, G>(g, a, fit, state + s.cur * Layout<MODEL>::K);
             g.sync();
             fit = -1;
         }
@@ -269,28 +204,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) lm_kernel(FitArgs a) {
 constexpr int kCovBlock = 128;
 
 template <int MODEL> __global__ void __launch_bounds__(kCovBlock) covariance_kernel(FitArgs a) {
-    constexpr int P = Model<MODEL>::P;
     const long long fit = (long long)blockIdx.x * kCovBlock + threadIdx.x;
-    if (fit >= a.n)
-        return;
-    float p[P], info[P * P], se[P];
-#pragma unroll
-    for (int k = 0; k < P; ++k)
-        p[k] = a.params[fit * P + k];
-    const int status = a.status[fit];
-    if (status == kConverged) {
-#pragma unroll
-        for (int k = 0; k < P * P; ++k)
-            info[k] = a.covariance[fit * P * P + k];
-    }
-    const int us = covariance_one<MODEL>(a, p, status, a.chi2[fit], info, se);
-#pragma unroll
-    for (int k = 0; k < P * P; ++k)
-        a.covariance[fit * P * P + k] = info[k];
-#pragma unroll
-    for (int k = 0; k < P; ++k)
-        a.stderr_out[fit * P + k] = se[k];
-    a.ustatus[fit] = us;
+    if (fit < a.n)
+        covariance_fit<MODEL>(a, fit);
 }
 
 // ------------------------------------------------ roofline microbenchmarks --

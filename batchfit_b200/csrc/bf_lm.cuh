@@ -555,4 +555,93 @@ __device__ int covariance_one(const FitArgs &a, const float *p, int fit_status, 
     return status;
 }
 
+// Outputs of a finished fit (FitResult, solver.hpp:43-48).
+template <int MODEL, int G>
+__device__ __forceinline__ void write_fit(const Group<G> &g, const FitArgs &a, long long fit, const LmState<MODEL> &s) {
+    constexpr int P = Model<MODEL>::P;
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        if (int(g.lane) == k)
+            a.params[fit * P + k] = s.p[k];
+    if (g.lane == 0) {
+        a.status[fit] = s.status;
+        a.iterations[fit] = s.iterations;
+        a.chi2[fit] = float(s.chi2);
+    }
+}
+
+// The accepted J^T J (the information matrix at the reported parameters), left in
+// the covariance output for the covariance kernel.
+template <int MODEL, int G>
+__device__ __forceinline__ void write_information(const Group<G> &g, const FitArgs &a, long long fit,
+                                                  const double *cur) {
+    constexpr int P = Model<MODEL>::P;
+    for (int k = int(g.lane); k < P * P; k += G) {
+        const int i = k / P, j = k % P;
+        a.covariance[fit * P * P + k] = float(cur[Layout<MODEL>::tri(i > j ? i : j, i > j ? j : i)]);
+    }
+}
+
+// Stage one fit-major y row into shared memory (kStore) or only scan it; reports
+// finiteness, flatness (every value equal to y[0]) and sum(y^2), with the same
+// arithmetic either way.
+template <int G, bool kStore = true>
+__device__ __forceinline__ void stage_row(const Group<G> &g, const float *row, int m, bool vec_ok, float *ys,
+                                          bool &yfin, bool &flat, float &syy) {
+    const float y0 = __ldg(row);
+    yfin = true;
+    flat = true;
+    syy = 0.0f;
+    if (vec_ok) {
+        const float4 *row4 = reinterpret_cast<const float4 *>(row);
+        for (int v = int(g.lane); v < m / 4; v += G) {
+            const float4 t = kStore ? __ldcs(row4 + v) : __ldg(row4 + v);
+            if constexpr (kStore)
+                reinterpret_cast<float4 *>(ys)[v] = t;
+            yfin = yfin && isfinite(t.x) && isfinite(t.y) && isfinite(t.z) && isfinite(t.w);
+            flat = flat && t.x == y0 && t.y == y0 && t.z == y0 && t.w == y0;
+            syy = fmaf(t.x, t.x, fmaf(t.y, t.y, fmaf(t.z, t.z, fmaf(t.w, t.w, syy))));
+        }
+    } else {
+        for (int j = int(g.lane); j < m; j += G) {
+            const float t = kStore ? __ldcs(row + j) : __ldg(row + j);
+            if constexpr (kStore)
+                ys[j] = t;
+            yfin = yfin && isfinite(t);
+            flat = flat && t == y0;
+            syy = fmaf(t, t, syy);
+        }
+    }
+    yfin = g.all(yfin);
+    flat = g.all(flat);
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1)
+        syy += g.xor_(syy, o);
+    g.sync();
+}
+
+// Covariance of one finished fit from the information matrix the LM kernel left in
+// its covariance slot: covariance, standard errors and the uncertainty status.
+template <int MODEL> __device__ __forceinline__ void covariance_fit(const FitArgs &a, long long fit) {
+    constexpr int P = Model<MODEL>::P;
+    float p[P], info[P * P], se[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        p[k] = a.params[fit * P + k];
+    const int status = a.status[fit];
+    if (status == kConverged) {
+#pragma unroll
+        for (int k = 0; k < P * P; ++k)
+            info[k] = a.covariance[fit * P * P + k];
+    }
+    const int us = covariance_one<MODEL>(a, p, status, a.chi2[fit], info, se);
+#pragma unroll
+    for (int k = 0; k < P * P; ++k)
+        a.covariance[fit * P * P + k] = info[k];
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        a.stderr_out[fit * P + k] = se[k];
+    a.ustatus[fit] = us;
+}
+
 } // namespace bf
