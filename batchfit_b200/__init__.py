@@ -25,8 +25,8 @@ import numpy as np
 from . import _capi
 
 __version__ = "0.1.0"
-__all__ = ["fit", "FitResult", "FitResultWithUncertainties", "FitStatus", "UncertaintyStatus", "cuda_available",
-           "MODELS", "__version__"]
+__all__ = ["fit", "fit_batch", "autotune", "FitResult", "FitResultWithUncertainties", "FitStatus",
+           "UncertaintyStatus", "cuda_available", "MODELS", "__version__"]
 
 MODELS = {"gaussian": 0, "lorentzian": 1, "pseudo_voigt": 2, "two_lorentzian": 3}
 _PARAMETERS = {"gaussian": 3, "lorentzian": 3, "pseudo_voigt": 4, "two_lorentzian": 8}
@@ -191,7 +191,8 @@ def fit(x, y, model="lorentzian", p0=None, bounds=None, device="auto", *, uncert
     return FitResult(params, status, iterations, chi2)
 
 
-def _fit_device(x, y, model, p0, bounds, uncertainties, policy, group_lanes, options):
+def _device_segment(x, y, model, p0, bounds, uncertainties, policy, group_lanes, options):
+    """Validate torch CUDA inputs and allocate outputs -> (FitArgs, FitOutputs, result, keep-alive)."""
     import torch  # device-memory inputs come from torch (plumbing only)
 
     if not (isinstance(x, torch.Tensor) and isinstance(y, torch.Tensor)):
@@ -216,8 +217,6 @@ def _fit_device(x, y, model, p0, bounds, uncertainties, policy, group_lanes, opt
         p0 = p0.contiguous()
     lower, upper = _bounds(bounds, p)
     opts = options if options is not None else solver_options(model, lower, upper, policy)
-    device_index = y.device.index or 0
-    ctx = context(device_index)
     kw = dict(device=y.device)
     params = torch.empty((n, p), dtype=torch.float32, **kw)
     status = torch.empty(n, dtype=torch.int32, **kw)
@@ -230,11 +229,78 @@ def _fit_device(x, y, model, p0, bounds, uncertainties, policy, group_lanes, opt
     args = _capi.FitArgs(MODELS[model], n, x.numel(), ptr(x), ptr(y), ptr(p0), _capi.BF_MEMORY_DEVICE,
                          int(uncertainties), int(group_lanes), opts)
     outs = _capi.FitOutputs(ptr(params), ptr(status), ptr(iterations), ptr(chi2), ptr(cov), ptr(se), ptr(us))
-    torch.cuda.current_stream(y.device).synchronize()
-    ctx.fit(args, outs)
     if uncertainties:
-        return FitResultWithUncertainties(params, status, iterations, chi2, cov, se, us)
-    return FitResult(params, status, iterations, chi2)
+        result = FitResultWithUncertainties(params, status, iterations, chi2, cov, se, us)
+    else:
+        result = FitResult(params, status, iterations, chi2)
+    return args, outs, result, (x, y, p0)
+
+
+def _fit_device(x, y, model, p0, bounds, uncertainties, policy, group_lanes, options):
+    import torch
+
+    args, outs, result, keep = _device_segment(x, y, model, p0, bounds, uncertainties, policy, group_lanes, options)
+    device = keep[1].device
+    torch.cuda.current_stream(device).synchronize()
+    context(device.index or 0).fit(args, outs)
+    return result
+
+
+def fit_batch(requests, *, fixed_mapping=False, graph=True):
+    """Fit many independent requests of different models and M as one mixed batch.
+
+    Each request is a dict with the arguments of ``fit``: ``x``, ``y``, and
+    optionally ``model``, ``p0``, ``bounds``, ``uncertainties``, ``policy``,
+    ``group_lanes`` and ``options``.  x/y may be numpy arrays (copied to the GPU)
+    or torch CUDA tensors.  Returns one result per request, in order, as torch CUDA
+    tensors.  All requests run in one persistent launch per kernel; each result is
+    the one ``fit`` gives for the same request alone with the same lanes per fit.
+    ``fixed_mapping`` runs every fit on one warp in request order (the plain
+    mapping); ``graph=False`` launches the kernels one by one.
+    """
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("CUDA fitting is unavailable: no CUDA device")
+    segments, results, keep = [], [], []
+    device = None
+    for i, req in enumerate(requests):
+        req = dict(req)
+        model = req.pop("model", "lorentzian")
+        if model not in _PARAMETERS:
+            raise ValueError(f"request {i}: unknown model {model!r}")
+        x, y = req.pop("x"), req.pop("y")
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        if not _is_device(x):
+            x = torch.as_tensor(np.ascontiguousarray(_real_array(x, "x"), dtype=np.float32)).to(dev)
+        if not _is_device(y):
+            y = torch.as_tensor(np.ascontiguousarray(_real_array(y, "y"), dtype=np.float32)).to(dev)
+        device = device or y.device
+        p0 = req.pop("p0", None)
+        unc = req.pop("uncertainties", False)
+        if not isinstance(unc, (bool, np.bool_)):
+            raise TypeError(f"request {i}: uncertainties must be a boolean")
+        args, outs, result, k = _device_segment(x, y, model, p0, req.pop("bounds", None), bool(unc),
+                                                req.pop("policy", "parity"), req.pop("group_lanes", 0),
+                                                req.pop("options", None))
+        if req:
+            raise TypeError(f"request {i}: unexpected keys {sorted(req)}")
+        segments.append(_capi.BatchSegment(args, outs))
+        results.append(result)
+        keep.append(k)
+    if not segments:
+        return []
+    torch.cuda.current_stream(device).synchronize()
+    flags = (_capi.BF_BATCH_FIXED_MAPPING if fixed_mapping else 0) | (0 if graph else _capi.BF_BATCH_NO_GRAPH)
+    context(device.index or 0).fit_batch(segments, flags)
+    return results
+
+
+def autotune(device: int = 0):
+    """Time the LM kernel per (model, M bucket) at 8/16/32 lanes per fit on the
+    device and keep the fastest for later mixed batches; returns lanes[4][8]."""
+    t = context(device).autotune()
+    return [[t.lanes[m][b] for b in range(8)] for m in range(4)]
 
 
 def guess(x, y, model="lorentzian"):

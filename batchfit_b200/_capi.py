@@ -29,8 +29,12 @@ EXPORTS = (
     "bf_cuda_last_error", "bf_cuda_available", "bf_cuda_version", "bf_cuda_context_create",
     "bf_cuda_context_destroy", "bf_cuda_default_options", "bf_cuda_fit", "bf_cuda_submit", "bf_cuda_ready",
     "bf_cuda_wait", "bf_cuda_guess", "bf_cuda_last_timing", "bf_cuda_host_alloc", "bf_cuda_host_free",
-    "bf_cuda_max_points", "bf_cuda_measure_peaks", "bf_cuda_fit_noalloc",
+    "bf_cuda_max_points", "bf_cuda_measure_peaks", "bf_cuda_fit_noalloc", "bf_cuda_fit_batch",
+    "bf_cuda_batch_max_points", "bf_cuda_autotune", "bf_cuda_get_tuning", "bf_cuda_set_tuning",
 )
+
+BF_BATCH_FIXED_MAPPING = 1
+BF_BATCH_NO_GRAPH = 2
 
 
 class SolverOptions(C.Structure):
@@ -97,6 +101,14 @@ class Timing(C.Structure):
     ]
 
 
+class BatchSegment(C.Structure):
+    _fields_ = [("args", FitArgs), ("out", FitOutputs)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("lanes", (C.c_int32 * 8) * 4), ("lm_ms", ((C.c_double * 3) * 8) * 4), ("tuned", C.c_int32)]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -131,6 +143,11 @@ def load():
         lib.bf_cuda_max_points.restype = C.c_uint32
         lib.bf_cuda_measure_peaks.argtypes = [vp, C.POINTER(Peaks)]
         lib.bf_cuda_fit_noalloc.argtypes = [C.POINTER(FitArgs), C.POINTER(FitOutputs), vp]
+        lib.bf_cuda_fit_batch.argtypes = [vp, C.POINTER(BatchSegment), C.c_uint32, C.c_uint32]
+        lib.bf_cuda_batch_max_points.restype = C.c_uint32
+        lib.bf_cuda_autotune.argtypes = [vp, C.POINTER(Tuning)]
+        lib.bf_cuda_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        lib.bf_cuda_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
         for name in EXPORTS:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
         _lib = lib
@@ -206,6 +223,24 @@ class Context:
         p = Peaks()
         check(self._lib.bf_cuda_measure_peaks(self._ptr, C.byref(p)), "bf_cuda_measure_peaks")
         return p
+
+    def fit_batch(self, segments, flags: int = 0):
+        """Run a list of BatchSegment (device pointers) as one mixed batch."""
+        arr = (BatchSegment * max(1, len(segments)))(*segments)
+        check(self._lib.bf_cuda_fit_batch(self._ptr, arr, len(segments), flags), "bf_cuda_fit_batch")
+
+    def autotune(self) -> Tuning:
+        t = Tuning()
+        check(self._lib.bf_cuda_autotune(self._ptr, C.byref(t)), "bf_cuda_autotune")
+        return t
+
+    def get_tuning(self) -> Tuning:
+        t = Tuning()
+        check(self._lib.bf_cuda_get_tuning(self._ptr, C.byref(t)), "bf_cuda_get_tuning")
+        return t
+
+    def set_tuning(self, t: Tuning):
+        check(self._lib.bf_cuda_set_tuning(self._ptr, C.byref(t)), "bf_cuda_set_tuning")
 
     def timing(self) -> Timing:
         t = Timing()

@@ -1,0 +1,341 @@
+// Persistent kernels of a mixed batch (bf_batch.h): spectra of uneven M and mixed
+// models in one launch per kernel, fed from a device work queue.
+//
+// Spectra are not staged in shared memory: with uneven M no fixed per-group buffer
+// fits every fit, so the kernels read x and y through the L1 cache (read-only
+// loads).  A fit's working set (its y row and x grid) stays resident in L1/L2 for
+// the passes of its LM iterations; y comes from HBM once per kernel.
+//
+// Every warp walks the class list in order.  For each class it runs the class's
+// template instantiation: its groups claim work items through the class's atomic
+// counter until the class is drained, then the warp moves on.  There is no
+// block-wide synchronisation, so warps drift between classes freely.
+#include "bf_batch.cuh"
+
+#include <mutex>
+
+namespace bf {
+
+namespace {
+
+// Grid constants of one segment's x grid, computed by one warp: the same values
+// cta_prologue derives for a CTA-staged grid (solver.hpp:58-69,223-239;
+// initial_guess.hpp:131-153).
+__device__ XConst xconst_warp(const float *x, int m) {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned min_abs = 0x7f800000u, min_diff = 0x7f800000u;
+    bool fin = true, up = true, down = true, strict = true, varied = false;
+    const float x0 = __ldg(x);
+    for (int j = int(lane); j < m; j += 32) {
+        const float v = __ldg(x + j);
+        fin = fin && isfinite(v);
+        varied = varied || v != x0;
+        if (j > 0) {
+            const float prev = __ldg(x + j - 1);
+            const float d = v - prev;
+            up = up && d >= 0.0f;
+            down = down && d <= 0.0f;
+            if (d != 0.0f && isfinite(d))
+                min_abs = min(min_abs, __float_as_uint(fabsf(d)));
+            strict = strict && v > prev;
+            if (d > 0.0f)
+                min_diff = min(min_diff, __float_as_uint(d));
+        }
+    }
+    XConst xc;
+    fin = __all_sync(0xffffffffu, fin);
+    up = __all_sync(0xffffffffu, up);
+    down = __all_sync(0xffffffffu, down);
+    strict = __all_sync(0xffffffffu, strict);
+    varied = __any_sync(0xffffffffu, varied);
+    min_abs = __reduce_min_sync(0xffffffffu, min_abs);
+    min_diff = __reduce_min_sync(0xffffffffu, min_diff);
+    xc.m = m;
+    xc.x_finite = fin;
+    xc.varied_x = varied;
+    const float spacing = __uint_as_float(min_abs);
+    xc.spacing = (up || down) && isfinite(spacing) ? spacing : 0.0f;
+    const int count = edge_count(m);
+    xc.count = count;
+    xc.n1 = pow2_at_least(count);
+    xc.guess_ok = m >= 5 && fin && strict && isfinite(rsub(__ldg(x + m - 1), x0));
+    xc.guess_spacing = __uint_as_float(min_diff);
+    xc.left_x = midpoint_rn(__ldg(x + (count - 1) / 2), __ldg(x + count / 2));
+    xc.right_x = midpoint_rn(__ldg(x + m - count + (count - 1) / 2), __ldg(x + m - count + count / 2));
+    return xc;
+}
+
+// Per segment: the x-grid constants.  Per run: one work item per fit.
+__global__ void __launch_bounds__(kBatchBlock) batch_prepare_kernel(BatchArgs b) {
+    const BatchHeader h = *b.hdr;
+    const int warp = int(blockIdx.x) * kBatchWarps + int(threadIdx.x / 32);
+    const int warps = int(gridDim.x) * kBatchWarps;
+    for (int s = warp; s < h.segments; s += warps) {
+        const XConst xc = xconst_warp(b.segs[s].a.x, b.segs[s].a.m);
+        if ((threadIdx.x & 31u) == 0u)
+            b.segs[s].xc = xc;
+    }
+    const int runs = h.lm_runs + h.guess_runs;
+    for (int r = int(blockIdx.x); r < runs; r += int(gridDim.x)) {
+        const bool lm = r < h.lm_runs;
+        const WorkRun run = lm ? b.lm_runs[r] : b.guess_runs[r - h.lm_runs];
+        WorkItem *items = lm ? b.lm_items : b.guess_items;
+        for (long long i = threadIdx.x; i < run.count; i += kBatchBlock)
+            items[run.start + i] = WorkItem{run.segment, int(run.first + i)};
+    }
+}
+
+// --------------------------------------------------------------------- LM --
+// The round loop of lm_kernel over a class's items: one fused pass per round,
+// then the FP64 control; a finished group claims its next item.
+template <int MODEL, int G>
+__device__ __forceinline__ void lm_class(const BatchArgs &b, const WorkClass &cls, unsigned long long *counter,
+                                         double *state) {
+    constexpr int P = Model<MODEL>::P;
+    constexpr int K = Layout<MODEL>::K;
+    const Group<G> g;
+    LmState<MODEL> s;
+    const Segment *seg = nullptr;
+    const float *row = nullptr;
+    int fit = -1;
+    bool flat = false;
+    float syy = 0.0f;
+    while (true) {
+        if (fit < 0) {
+            // Intake: claim items until one needs a pass or the class is drained.
+            WorkItem it;
+            while (claim(g, counter, cls, b.lm_items, it)) {
+                seg = &b.segs[it.segment];
+                const FitArgs &a = seg->a;
+                const int m = a.m;
+                row = a.y + (long long)it.fit * m;
+                const bool vec_ok = (m & 3) == 0 && (reinterpret_cast<uintptr_t>(row) & 15) == 0;
+                bool yfin;
+                stage_row<G, false>(g, row, m, vec_ok, nullptr, yfin, flat, syy);
+                bool init_finite = true;
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    s.p[k] = a.p0[(long long)it.fit * P + k];
+                    init_finite = init_finite && isfinite(s.p[k]);
+                }
+                if (a.options_ok && init_finite && seg->xc.x_finite && yfin) {
+                    lm_begin<MODEL>(a, s);
+                    fit = it.fit;
+                    break;
+                }
+                // Preflight rejection (solver.hpp:205-226): parameters keep the initial values.
+                s.status = kInvalid;
+                s.iterations = 0;
+                s.chi2 = __longlong_as_double(0x7ff8000000000000ll);
+                write_fit<MODEL, G>(g, a, it.fit, s);
+            }
+            if (fit < 0)
+                break;
+        }
+        const FitArgs &a = seg->a;
+        const XConst xc = seg->xc;
+        const bool pass_finite = lm_pass<MODEL, G>(g, a.x, row, a.m, s.t, state + (1 - s.cur) * K);
+        bool done = lm_after_pass<MODEL, G>(g, a, xc, flat, pass_finite, state, s);
+        if (!done)
+            done = lm_plan<MODEL>(a, xc, double(syy), state, s);
+        if (done) {
+            write_fit<MODEL, G>(g, a, fit, s);
+            if (a.uncertainties && s.status == kConverged)
+                write_information<MODEL, G>(g, a, fit, state + s.cur * K);
+            g.sync();
+            fit = -1;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBatchBlock, kBatchMinBlocks) batch_lm_kernel(BatchArgs b) {
+    extern __shared__ __align__(16) double lm_smem[];
+    double *warp_state = lm_smem + (threadIdx.x / 32) * kLmWarpDoubles;
+    const int classes = b.hdr->lm_classes;
+    for (int c = 0; c < classes; ++c) {
+        const WorkClass cls = b.lm_classes[c];
+        const int group = int(threadIdx.x & 31u) / cls.lanes;
+        double *state = warp_state + group * kLmSlotDoubles;
+        switch (cls.model * 100 + cls.lanes) {
+#define BF_LM_CASE(MODEL, G)                                                                                   \
+    case MODEL * 100 + G: lm_class<MODEL, G>(b, cls, b.counters + c, state); break;
+#define BF_LM_MODEL(MODEL) BF_LM_CASE(MODEL, 8) BF_LM_CASE(MODEL, 16) BF_LM_CASE(MODEL, 32)
+            BF_LM_MODEL(0)
+            BF_LM_MODEL(1)
+            BF_LM_MODEL(2)
+            BF_LM_MODEL(3)
+#undef BF_LM_MODEL
+#undef BF_LM_CASE
+        default: break;
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------- covariance --
+// One thread per LM work item; items of segments without uncertainties are skipped.
+__global__ void __launch_bounds__(128) batch_covariance_kernel(BatchArgs b) {
+    if (b.hdr->uncertain_segments == 0)
+        return;
+    const long long items = b.hdr->lm_items;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < items;
+         t += (long long)gridDim.x * blockDim.x) {
+        const WorkItem it = b.lm_items[t];
+        const Segment &seg = b.segs[it.segment];
+        if (!seg.a.uncertainties)
+            continue;
+        switch (seg.model) {
+        case kGaussian: covariance_fit<kGaussian>(seg.a, it.fit); break;
+        case kLorentzian: covariance_fit<kLorentzian>(seg.a, it.fit); break;
+        case kPseudoVoigt: covariance_fit<kPseudoVoigt>(seg.a, it.fit); break;
+        default: covariance_fit<kTwoLorentzian>(seg.a, it.fit); break;
+        }
+    }
+}
+
+// ------------------------------------------------------------- synthetic --
+// Counter-based uniform in (0, 1): SplitMix64 finaliser of (seed, stream, index).
+__device__ __forceinline__ float uniform01(unsigned seed, unsigned long long stream, unsigned long long index) {
+    unsigned long long z = (static_cast<unsigned long long>(seed) << 32) ^ (stream * 0x9e3779b97f4a7c15ull) ^ index;
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    return (float(z >> 40) + 0.5f) * (1.0f / 16777216.0f);
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(256) synthetic_kernel(int m, long long n, unsigned seed, float *x, float *y) {
+    constexpr int P = Model<MODEL>::P;
+    const long long total = n * m;
+    const float dx = 20.0f / float(m > 1 ? m - 1 : 1);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long fit = t / m;
+        const int j = int(t - fit * m);
+        const float xj = j == m - 1 ? 10.0f : -10.0f + dx * float(j);
+        if (fit == 0)
+            x[j] = xj;
+        auto u = [&](int k) { return uniform01(seed, (unsigned long long)fit, (unsigned long long)(k)); };
+        const float amp = 0.5f + 4.5f * u(0);
+        const float center = -6.0f + 12.0f * u(1);
+        const float fwhm = 0.1f * __expf(u(2) * __logf(30.0f));
+        float p[8] = {amp, center, fwhm, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if constexpr (MODEL == kGaussian)
+            p[2] = fwhm / 2.354820045f;
+        else if constexpr (MODEL == kLorentzian)
+            p[2] = 0.5f * fwhm;
+        else if constexpr (MODEL == kPseudoVoigt)
+            p[3] = u(3);
+        else {
+            const float w2 = 0.2f * __expf(u(4) * __logf(10.0f));
+            p[2] = 0.5f * fwhm;
+            p[3] = amp * (0.1f + 0.9f * u(5));
+            p[4] = center + (0.5f + 2.5f * u(6)) * 0.5f * (p[2] + w2);
+            p[5] = w2;
+        }
+        const auto q = Model<MODEL>::prepare(p);
+        float J[P];
+        const float f = -Model<MODEL>::residual(q, xj, 0.0f, J);
+        const float u1 = uniform01(seed, (unsigned long long)fit, 1000ull + 2ull * j);
+        const float u2 = uniform01(seed, (unsigned long long)fit, 1001ull + 2ull * j);
+        const float noise = sqrtf(-2.0f * __logf(u1)) * __cosf(6.283185307f * u2);
+        y[t] = f + 0.01f * amp * noise;
+    }
+}
+
+struct Grids {
+    int device = -1;
+    int guess = 0, lm = 0;
+};
+
+// Grids per device, resolved once (outside any stream capture: the first batch
+// on a context launches directly).
+cudaError_t grids_for(int sms, Grids &out) {
+    constexpr int kDevices = 64;
+    static Grids cache[kDevices];
+    static std::mutex mutex;
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess)
+        return e;
+    if (device < 0 || device >= kDevices)
+        return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mutex);
+    if (cache[device].device == device) {
+        out = cache[device];
+        return cudaSuccess;
+    }
+    int per_sm_guess = 0, per_sm_lm = 0;
+    e = batch_guess_blocks_per_sm(&per_sm_guess);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(batch_lm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kLmSmem);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_lm, batch_lm_kernel, kBatchBlock, kLmSmem);
+    if (e != cudaSuccess)
+        return e;
+    Grids g;
+    g.device = device;
+    g.guess = sms * (per_sm_guess > 0 ? per_sm_guess : 1);
+    g.lm = sms * (per_sm_lm > 0 ? per_sm_lm : 1);
+    cache[device] = g;
+    out = g;
+    return cudaSuccess;
+}
+
+} // namespace
+
+bool batch_guess_shape(int m, int *lanes, int *v) {
+    const int n1 = pow2_at_least(edge_count(m));
+    if (n1 <= 32) {
+        *lanes = 8;
+        *v = 4;
+    } else if (n1 <= 128) {
+        *lanes = 8;
+        *v = 16;
+    } else if (n1 <= 256) {
+        *lanes = 16;
+        *v = 16;
+    } else if (n1 <= 512) {
+        *lanes = 32;
+        *v = 16;
+    } else {
+        *lanes = 32;
+        *v = 0;
+    }
+    return n1 <= kBatchMaxSortWidth;
+}
+
+cudaError_t launch_synthetic(int model, int m, long long n, unsigned seed, float *x, float *y,
+                             cudaStream_t stream) {
+    const unsigned grid = 148u * 16u;
+    switch (model) {
+    case kGaussian: synthetic_kernel<kGaussian><<<grid, 256, 0, stream>>>(m, n, seed, x, y); break;
+    case kLorentzian: synthetic_kernel<kLorentzian><<<grid, 256, 0, stream>>>(m, n, seed, x, y); break;
+    case kPseudoVoigt: synthetic_kernel<kPseudoVoigt><<<grid, 256, 0, stream>>>(m, n, seed, x, y); break;
+    default: synthetic_kernel<kTwoLorentzian><<<grid, 256, 0, stream>>>(m, n, seed, x, y); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_pipeline(const BatchArgs &b, int sms, cudaStream_t stream, cudaEvent_t guessed,
+                                  cudaEvent_t fitted) {
+    Grids grids;
+    cudaError_t e = grids_for(sms, grids);
+    if (e != cudaSuccess)
+        return e;
+    e = cudaMemsetAsync(b.counters, 0, 2 * kMaxClasses * sizeof(unsigned long long), stream);
+    if (e != cudaSuccess)
+        return e;
+    batch_prepare_kernel<<<sms * 4, kBatchBlock, 0, stream>>>(b);
+    launch_batch_guess(b, grids.guess, stream);
+    if (guessed && (e = cudaEventRecord(guessed, stream)) != cudaSuccess)
+        return e;
+    batch_lm_kernel<<<grids.lm, kBatchBlock, kLmSmem, stream>>>(b);
+    if (fitted && (e = cudaEventRecord(fitted, stream)) != cudaSuccess)
+        return e;
+    batch_covariance_kernel<<<sms * 8, 128, 0, stream>>>(b);
+    return cudaGetLastError();
+}
+
+} // namespace bf

@@ -6,6 +6,7 @@
 // copied in, fitted and copied out on stream c % 2, so the copies of one chunk
 // overlap the kernel of the other.
 #include "batchfit_cuda.h"
+#include "bf_context.h"
 #include "bf_kernels.h"
 
 #include <algorithm>
@@ -17,6 +18,11 @@
 #include <mutex>
 #include <string>
 #include <vector>
+
+using bf::host::DeviceBuffer;
+using bf::host::KernelEvents;
+using bf::host::kSlots;
+using bf::host::Slot;
 
 namespace {
 
@@ -40,67 +46,14 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 int parameter_count(int model) { return model == 2 ? 4 : model == 3 ? 8 : 3; }
 
-struct DeviceBuffer {
-    void *ptr = nullptr;
-    size_t bytes = 0;
-    cudaError_t reserve(size_t need) {
-        if (need <= bytes)
-            return cudaSuccess;
-        if (ptr)
-            cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-        const cudaError_t e = cudaMalloc(&ptr, need);
-        if (e == cudaSuccess)
-            bytes = need;
-        return e;
-    }
-    void release() {
-        if (ptr)
-            cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-    }
-};
-
-// Device-side storage of one in-flight chunk.
-struct Slot {
-    DeviceBuffer y, p0, guess, params, status, iterations, chi2, cov, se, ustatus, counter;
-};
-
 // Guess-only outputs (bf_cuda_guess); null members in a fit.
 struct GuessOnly {
     float *params;
     int32_t *status;
 };
 
-constexpr int kSlots = 2;
 
 } // namespace
-
-// Events around the kernels of one batch: guess = [start, guessed), LM =
-// [guessed, fitted), covariance = [fitted, done).
-struct KernelEvents {
-    cudaEvent_t start, guessed, fitted, done;
-};
-
-struct bf_cuda_context {
-    int device = 0;
-    int sms = 0;
-    std::mutex mutex;
-    std::atomic<bool> busy{false};
-    cudaStream_t stream[kSlots] = {nullptr, nullptr};
-    cudaEvent_t start = nullptr, stop = nullptr, joined = nullptr;
-    DeviceBuffer x;
-    Slot slot[kSlots];
-    bf_cuda_timing last{};
-    // Kernel events of the in-flight submission (one set per chunk).
-    std::vector<KernelEvents> kernel_events;
-    std::vector<cudaEvent_t> event_pool;
-    int launches = 0;
-    int lanes = 0;
-    bf::LaunchInfo info{};
-};
 
 struct bf_cuda_pending {
     bf_cuda_context *ctx;
@@ -169,7 +122,8 @@ bf::FitArgs make_args(const bf_fit_args &in, int p) {
     return a;
 }
 
-int validate(const bf_fit_args *args, const bf_fit_outputs *out) {
+// limit == 0: the largest M of the shared-memory kernels for the model.
+int validate(const bf_fit_args *args, const bf_fit_outputs *out, uint32_t limit = 0) {
     if (!args || !out)
         return fail(BF_ERR_INVALID_ARGUMENT, "null argument block");
     if (args->model < 0 || args->model > 3)
@@ -178,7 +132,8 @@ int validate(const bf_fit_args *args, const bf_fit_outputs *out) {
         return fail(BF_ERR_INVALID_ARGUMENT, "fit requires nonempty x[M] (M > 0)");
     if (args->memory != BF_MEMORY_HOST && args->memory != BF_MEMORY_DEVICE)
         return fail(BF_ERR_INVALID_ARGUMENT, "memory must be BF_MEMORY_HOST or BF_MEMORY_DEVICE");
-    const uint32_t limit = uint32_t(bf::max_points(args->model));
+    if (limit == 0)
+        limit = uint32_t(bf::max_points(args->model));
     if (args->m > limit)
         return fail(BF_ERR_INVALID_ARGUMENT,
                     "M=" + std::to_string(args->m) + " exceeds this backend's limit of " + std::to_string(limit));
@@ -402,6 +357,14 @@ int prepare(const bf_fit_args *args, const bf_fit_outputs *out, FitArgs *base, i
     *lanes = choose_lanes(args->model, args->m, args->group_lanes);
     return BF_OK;
 }
+int prepare_segment(const bf_fit_args *args, const bf_fit_outputs *out, uint32_t max_points, FitArgs *base) {
+    const int rc = validate(args, out, max_points);
+    if (rc != BF_OK)
+        return rc;
+    *base = make_args(*args, parameter_count(args->model));
+    return BF_OK;
+}
+int default_lanes(int model, uint32_t m) { return choose_lanes(model, m, 0); }
 int report(int code, const std::string &message) { return fail(code, message); }
 int report_cuda(cudaError_t e, const char *what) { return cuda_fail(e, what); }
 } // namespace host
@@ -490,6 +453,8 @@ void bf_cuda_context_destroy(bf_cuda_context *ctx) {
         s.counter.release();
     }
     ctx->x.release();
+    bf::host::release_batch_state(ctx->batch);
+    ctx->batch = nullptr;
     for (auto &ev : ctx->kernel_events)
         for (cudaEvent_t e : {ev.start, ev.guessed, ev.fitted, ev.done})
             cudaEventDestroy(e);

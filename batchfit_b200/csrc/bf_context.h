@@ -1,0 +1,88 @@
+// Host-side state of a bf_cuda_context, shared by the C ABI translation units.
+#pragma once
+
+#include "batchfit_cuda.h"
+#include "bf_args.h"
+
+#include <atomic>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace bf {
+namespace host {
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t need) {
+        if (need <= bytes)
+            return cudaSuccess;
+        if (ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        const cudaError_t e = cudaMalloc(&ptr, need);
+        if (e == cudaSuccess)
+            bytes = need;
+        return e;
+    }
+    void release() {
+        if (ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+// Device-side storage of one in-flight chunk.
+struct Slot {
+    DeviceBuffer y, p0, guess, params, status, iterations, chi2, cov, se, ustatus, counter;
+};
+
+constexpr int kSlots = 2;
+
+struct BatchState; // mixed-batch arena and graph (bf_batch.cu)
+void release_batch_state(BatchState *state);
+
+// Shared by the C ABI translation units (bf_capi.cu).
+int prepare(const bf_fit_args *args, const bf_fit_outputs *out, FitArgs *base, int *lanes);
+// Checks of one mixed-batch segment (M up to max_points) and its kernel arguments.
+int prepare_segment(const bf_fit_args *args, const bf_fit_outputs *out, uint32_t max_points, FitArgs *base);
+// Group width the single-batch path picks for (model, M).
+int default_lanes(int model, uint32_t m);
+int report(int code, const std::string &message);
+int report_cuda(cudaError_t e, const char *what);
+// Mixed batches (bf_batch.cu): plan, upload and run synchronously on stream[0].
+int run_batch(bf_cuda_context *ctx, const bf_batch_segment *segments, uint32_t count, uint32_t flags);
+int batch_state(bf_cuda_context *ctx, BatchState **out);
+bf_tuning &tuning_of(BatchState *st);
+
+// Events around the kernels of one batch: guess = [start, guessed), LM =
+// [guessed, fitted), covariance = [fitted, done).
+struct KernelEvents {
+    cudaEvent_t start, guessed, fitted, done;
+};
+
+} // namespace host
+} // namespace bf
+
+struct bf_cuda_context {
+    int device = 0;
+    int sms = 0;
+    std::mutex mutex;
+    std::atomic<bool> busy{false};
+    cudaStream_t stream[bf::host::kSlots] = {nullptr, nullptr};
+    cudaEvent_t start = nullptr, stop = nullptr, joined = nullptr;
+    bf::host::DeviceBuffer x;
+    bf::host::Slot slot[bf::host::kSlots];
+    bf_cuda_timing last{};
+    // Kernel events of the in-flight submission (one set per chunk).
+    std::vector<bf::host::KernelEvents> kernel_events;
+    std::vector<cudaEvent_t> event_pool;
+    int launches = 0;
+    int lanes = 0;
+    bf::LaunchInfo info{};
+    bf::host::BatchState *batch = nullptr; // created by the first mixed batch
+};
+

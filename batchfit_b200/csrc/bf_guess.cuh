@@ -299,39 +299,34 @@ __device__ PeakFeature find_peak(const Group<G> &g, const Signal<MODEL> &s, cons
     return r;
 }
 
-// detail::prominence (initial_guess.hpp:38-54): walk outwards while the smoothed
-// signal stays at or below the start height, tracking the minimum on each side.
-template <int MODEL, int G>
-__device__ float prominence(const Group<G> &g, const Signal<MODEL> &s, int index) {
+// detail::prominence(signal, index) > threshold (initial_guess.hpp:38-54), by one
+// lane.  The reference walks outwards on each side while the smoothed signal stays
+// at or below the start height, takes the side minima and returns height minus the
+// larger minimum.  Rounding is monotone, so that exceeds the threshold iff on both
+// sides some sample of the walk has height - sample > threshold: each walk stops
+// at its first such sample (side passes) or at the reference's stop (side fails).
+template <int MODEL> __device__ bool prominent(const Signal<MODEL> &s, int index, float threshold) {
     const float height = s.smooth(index);
-    float left = height, right = height;
-    for (int top = index - 1; top >= 0; top -= G) {
-        const int pos = top - int(g.lane);
-        const float v = pos >= 0 ? s.smooth(pos) : height;
-        const unsigned b = g.ballot(pos >= 0 && v > height);
-        const int stop = b ? __ffs(b) - 1 : G;
-        float mv = (int(g.lane) < stop && pos >= 0) ? v : height;
-#pragma unroll
-        for (int o = G / 2; o >= 1; o >>= 1)
-            mv = fminf(mv, g.xor_(mv, o));
-        left = smin(left, mv);
-        if (b)
+    bool left = false;
+    for (int j = index - 1; j >= 0; --j) {
+        const float v = s.smooth(j);
+        if (v > height)
             break;
-    }
-    for (int bot = index + 1; bot < s.m; bot += G) {
-        const int pos = bot + int(g.lane);
-        const float v = pos < s.m ? s.smooth(pos) : height;
-        const unsigned b = g.ballot(pos < s.m && v > height);
-        const int stop = b ? __ffs(b) - 1 : G;
-        float mv = (int(g.lane) < stop && pos < s.m) ? v : height;
-#pragma unroll
-        for (int o = G / 2; o >= 1; o >>= 1)
-            mv = fminf(mv, g.xor_(mv, o));
-        right = smin(right, mv);
-        if (b)
+        if (rsub(height, v) > threshold) {
+            left = true;
             break;
+        }
     }
-    return rsub(height, smax(left, right));
+    if (!left)
+        return false;
+    for (int j = index + 1; j < s.m; ++j) {
+        const float v = s.smooth(j);
+        if (v > height)
+            return false;
+        if (rsub(height, v) > threshold)
+            return true;
+    }
+    return false;
 }
 
 // initial_guess<float,Model> for the spectrum ys[0..m).  `scratch` holds 2*n1 floats.
@@ -476,41 +471,70 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         }
     } else {
         // Second peak (initial_guess.hpp:199-227): the tallest smoothed local maximum
-        // that is far enough from the first and prominent enough.  Candidates are
-        // visited from tallest to shortest; only the prominence test is expensive.
+        // (ties: smaller index) that is far enough from the first and prominent
+        // enough.  One sweep collects each lane's two best candidates.  The best of
+        // the lanes' second candidates is a cut-off: every candidate better than it
+        // is some lane's first, so the candidates at or above the cut-off are the
+        // true leaders.  Each lane tests its own leaders; the best passing one is the
+        // answer.  When all fail, a second sweep tests every candidate below the
+        // cut-off, each lane its own indices, and keeps the best passing one.
         const float separation =
             smax(rmul(3.0f, xc.guess_spacing), rmul(2.0f, smin(primary.left_radius, primary.right_radius)));
         const float threshold = rmul(3.0f, noise);
-        float bound_v = __int_as_float(0x7f800000);
-        int bound_j = -1;
+        auto far_enough = [&](int j) {
+            const int idx = s.raw_maximum(j);
+            const int bins = idx > first ? idx - first : first - idx;
+            return !(bins < 3 || fabsf(rsub(xs[idx], primary.center)) < separation);
+        };
         int second = m;
-        while (true) {
-            float bv = 0.0f;
-            int bj = m;
-            scan_smoothed<MODEL, G>(g, s, [&](int j, float v, float left, float right) {
-                if (!(v > 0.0f && v > left && v >= right))
-                    return;
-                if (!(v < bound_v || (v == bound_v && j > bound_j)))
-                    return;
+        float v1 = 0.0f, v2 = 0.0f;
+        int j1 = m, j2 = m;
+        scan_smoothed<MODEL, G>(g, s, [&](int j, float v, float left, float right) {
+            if (!(v > 0.0f && v > left && v >= right))
+                return;
+            if (!(v > v2 || (v == v2 && j < j2)))
+                return;
+            if (!far_enough(j))
+                return;
+            if (v > v1 || (v == v1 && j < j1)) {
+                v2 = v1;
+                j2 = j1;
+                v1 = v;
+                j1 = j;
+            } else {
+                v2 = v;
+                j2 = j;
+            }
+        });
+        float cut_v = v2;
+        int cut_j = j2;
+        argmax_pair(g, cut_v, cut_j); // cut_j == m: every candidate was collected
+        auto leader = [&](float v, int j) {
+            return j != m && (cut_j == m || v > cut_v || (v == cut_v && j <= cut_j));
+        };
+        const bool pass1 = leader(v1, j1) && prominent(s, j1, threshold);
+        const bool pass2 = !pass1 && leader(v2, j2) && prominent(s, j2, threshold);
+        float bv = pass1 ? v1 : pass2 ? v2 : 0.0f;
+        int bj = pass1 ? j1 : pass2 ? j2 : m;
+        argmax_pair(g, bv, bj);
+        if (bj == m && cut_j != m) {
+            for (int j = 1 + int(g.lane); j + 1 < m; j += G) {
+                const float v = s.smooth_interior(j);
+                if (!(v > 0.0f && (v < cut_v || (v == cut_v && j > cut_j))))
+                    continue;
                 if (!(v > bv || (v == bv && j < bj)))
-                    return;
-                const int idx = s.raw_maximum(j);
-                const int bins = idx > first ? idx - first : first - idx;
-                if (bins < 3 || fabsf(rsub(xs[idx], primary.center)) < separation)
-                    return;
+                    continue;
+                if (!(v > s.smooth(j - 1) && v >= s.smooth(j + 1)))
+                    continue;
+                if (!far_enough(j) || !prominent(s, j, threshold))
+                    continue;
                 bv = v;
                 bj = j;
-            });
-            argmax_pair(g, bv, bj);
-            if (bj == m)
-                break;
-            if (prominence<MODEL, G>(g, s, bj) > threshold) {
-                second = s.raw_maximum(bj);
-                break;
             }
-            bound_v = bv;
-            bound_j = bj;
+            argmax_pair(g, bv, bj);
         }
+        if (bj != m)
+            second = s.raw_maximum(bj);
         if (second == m)
             return kGuessInsufficient;
         if (first > second) {

@@ -155,6 +155,47 @@ int bf_cuda_host_free(void *ptr);
 /* Largest M the kernels support for `model` (shared-memory layout bound). */
 uint32_t bf_cuda_max_points(int32_t model);
 
+/* ---- Mixed batches --------------------------------------------------------
+ * Many fit calls of different models and M run together: one persistent launch
+ * per kernel (guess, LM, covariance) claims the fits of every segment from a
+ * device work queue.  A segment is exactly one bf_cuda_fit call (one model, one
+ * shared x[M], fit-major y[N*M], p0 or NULL, bounds, options, outputs), so each
+ * segment is the reference's fit_batch<Model> / _core.fit call
+ * (include/batchfit/metal/batch.hpp:268-310, python/bindings.cpp:200-207); the
+ * reference has no call that mixes them.  Every pointer is device memory
+ * (args.memory == BF_MEMORY_DEVICE); M may go up to bf_cuda_batch_max_points().
+ * args.group_lanes 0 takes the tuned lanes per fit for (model, M)
+ * (bf_cuda_autotune, else a built-in table); 8, 16 or 32 forces a width.
+ * Results of a segment do not depend on the other segments in the batch. */
+typedef struct bf_batch_segment {
+    bf_fit_args args;
+    bf_fit_outputs out;
+} bf_batch_segment;
+
+/* Flags of bf_cuda_fit_batch. */
+#define BF_BATCH_FIXED_MAPPING 1u /* the plain mapping: one fit per warp (32 lanes), segments in call order */
+#define BF_BATCH_NO_GRAPH 2u      /* launch the kernels one by one (per-kernel timing) instead of a graph replay */
+
+/* Synchronous: returns when every segment's outputs are written. */
+int bf_cuda_fit_batch(bf_cuda_context *ctx, const bf_batch_segment *segments, uint32_t count, uint32_t flags);
+uint32_t bf_cuda_batch_max_points(void);
+
+/* Lanes per fit by (model, M bucket); bucket b holds M nearest 64 * 2^b
+ * (b = 0..7: 64 ... 8192).  No counterpart in the reference, which maps one fit
+ * per thread or per SIMD-group by a compile-time choice
+ * (include/batchfit/metal/batch.hpp:268-310, KernelVariant). */
+typedef struct bf_tuning {
+    int32_t lanes[4][8];
+    double lm_ms[4][8][3]; /* measured LM-kernel time per (model, bucket, 8/16/32 lanes); 0 if untimed */
+    int32_t tuned;         /* 1 after bf_cuda_autotune or bf_cuda_set_tuning */
+} bf_tuning;
+/* Times the LM kernel for every (model, bucket) at 8, 16 and 32 lanes per fit on
+ * seeded synthetic spectra generated on the device and keeps the fastest width.
+ * Takes a few hundred milliseconds; later batches on the context use the result. */
+int bf_cuda_autotune(bf_cuda_context *ctx, bf_tuning *out);
+int bf_cuda_get_tuning(bf_cuda_context *ctx, bf_tuning *out);
+int bf_cuda_set_tuning(bf_cuda_context *ctx, const bf_tuning *in);
+
 /* A fit that allocates nothing.  No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: a host whose memory pool already owns
