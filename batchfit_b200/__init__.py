@@ -25,7 +25,7 @@ import numpy as np
 from . import _capi
 
 __version__ = "0.1.0"
-__all__ = ["fit", "fit_batch", "autotune", "FitResult", "FitResultWithUncertainties", "FitStatus",
+__all__ = ["fit", "fit_batch", "autotune", "Server", "FitResult", "FitResultWithUncertainties", "FitStatus",
            "UncertaintyStatus", "cuda_available", "MODELS", "__version__"]
 
 MODELS = {"gaussian": 0, "lorentzian": 1, "pseudo_voigt": 2, "two_lorentzian": 3}
@@ -294,6 +294,120 @@ def fit_batch(requests, *, fixed_mapping=False, graph=True):
     flags = (_capi.BF_BATCH_FIXED_MAPPING if fixed_mapping else 0) | (0 if graph else _capi.BF_BATCH_NO_GRAPH)
     context(device.index or 0).fit_batch(segments, flags)
     return results
+
+
+class _Ticket:
+    """One submitted request: ``done()``, ``result()`` (blocks), ``latency_ms``."""
+
+    def __init__(self, server, ticket, result, keep):
+        self._server, self._ticket, self._result, self._keep = server, ticket, result, keep
+        self._code = None
+        self.latency_ms = None
+
+    def done(self) -> bool:
+        if self._code is not None:
+            return True
+        rc = self._server._lib.bf_server_poll(self._server._ptr, self._ticket)
+        if rc < 0:
+            _capi.check(-rc, "bf_server_poll")
+        return rc == 1
+
+    def result(self):
+        if self._code is None:
+            latency = C.c_double()
+            self._code = self._server._lib.bf_server_wait(self._server._ptr, self._ticket, C.byref(latency))
+            self.latency_ms = latency.value
+            self._server._live.pop(self._ticket, None)
+        _capi.check(self._code, "server request")
+        return self._result
+
+
+class Server:
+    """Continuous-batching fit server on one GPU (native scheduler thread).
+
+    ``submit`` takes the arguments of ``fit`` (host arrays) and returns a ticket at
+    once; requests are admitted while their device buffers fit ``memory_budget``
+    bytes (0: 150 GB, capped by free memory), coalesced into mixed batches, and up
+    to two batches run at once.  ``max_batch_fits`` caps the fits of one launch.
+    """
+
+    def __init__(self, device=0, memory_budget=0, max_batch_fits=0, fixed_mapping=False, graph=True,
+                 max_in_flight=2):
+        self._lib = _capi.load()
+        self._ptr = C.c_void_p()
+        flags = (_capi.BF_BATCH_FIXED_MAPPING if fixed_mapping else 0) | (0 if graph else _capi.BF_BATCH_NO_GRAPH)
+        opt = _capi.ServerOptions(int(memory_budget), int(max_batch_fits), flags, int(max_in_flight))
+        _capi.check(self._lib.bf_server_create(device, C.byref(opt), C.byref(self._ptr)), "bf_server_create")
+        # Host buffers of every request that has not been collected: the scheduler
+        # reads the inputs at admission and writes the outputs at completion.
+        self._live = {}
+
+    def submit(self, x, y, model="lorentzian", p0=None, bounds=None, *, uncertainties=False, policy="parity",
+               options=None):
+        if model not in _PARAMETERS:
+            raise ValueError(f"unknown model {model!r}; choose one of {tuple(_PARAMETERS)}")
+        if not isinstance(uncertainties, (bool, np.bool_)):
+            raise TypeError("uncertainties must be a boolean")
+        x = np.ascontiguousarray(_real_array(x, "x"), dtype=np.float32)
+        y = np.ascontiguousarray(_real_array(y, "y"), dtype=np.float32)
+        if y.ndim == 1:
+            y = y.reshape(1, -1)
+        if x.ndim != 1 or not x.size or y.ndim != 2 or y.shape[1] != x.size:
+            raise ValueError("expected x[M] and y[N,M] with M>0")
+        n, p = y.shape[0], _PARAMETERS[model]
+        if p0 is not None:
+            p0 = _real_array(p0, "p0")
+            if p0.shape == (p,):
+                p0 = np.broadcast_to(p0, (n, p))
+            if p0.shape != (n, p):
+                raise ValueError(f"p0 must have shape [{p}] or [{n},{p}]")
+            p0 = np.ascontiguousarray(p0, dtype=np.float32)
+        lower, upper = _bounds(bounds, p)
+        opts = options if options is not None else solver_options(model, lower, upper, policy)
+        params = np.empty((n, p), np.float32)
+        status = np.empty(n, np.int32)
+        iterations = np.empty(n, np.uint32)
+        chi2 = np.empty(n, np.float32)
+        cov = np.empty((n, p, p), np.float32) if uncertainties else None
+        se = np.empty((n, p), np.float32) if uncertainties else None
+        us = np.empty(n, np.int32) if uncertainties else None
+        ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        args = _capi.FitArgs(MODELS[model], n, x.size, ptr(x), ptr(y), ptr(p0), _capi.BF_MEMORY_HOST,
+                             int(bool(uncertainties)), 0, opts)
+        outs = _capi.FitOutputs(ptr(params), ptr(status), ptr(iterations), ptr(chi2), ptr(cov), ptr(se), ptr(us))
+        ticket = C.c_uint64()
+        _capi.check(self._lib.bf_server_submit(self._ptr, C.byref(args), C.byref(outs), C.byref(ticket)),
+                    "bf_server_submit")
+        if uncertainties:
+            result = FitResultWithUncertainties(params, status, iterations, chi2, cov, se, us)
+        else:
+            result = FitResult(params, status, iterations, chi2)
+        self._live[ticket.value] = (x, y, p0, result)
+        return _Ticket(self, ticket.value, result, None)
+
+    def stats(self) -> dict:
+        st = _capi.ServerStats()
+        _capi.check(self._lib.bf_server_get_stats(self._ptr, C.byref(st)), "bf_server_get_stats")
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def close(self):
+        """Complete every submitted request, then release the server."""
+        if self._ptr:
+            self._lib.bf_server_destroy(self._ptr)
+            self._ptr = C.c_void_p()
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def autotune(device: int = 0):

@@ -31,6 +31,8 @@ EXPORTS = (
     "bf_cuda_wait", "bf_cuda_guess", "bf_cuda_last_timing", "bf_cuda_host_alloc", "bf_cuda_host_free",
     "bf_cuda_max_points", "bf_cuda_measure_peaks", "bf_cuda_fit_noalloc", "bf_cuda_fit_batch",
     "bf_cuda_batch_max_points", "bf_cuda_autotune", "bf_cuda_get_tuning", "bf_cuda_set_tuning",
+    "bf_server_create", "bf_server_destroy", "bf_server_submit", "bf_server_poll", "bf_server_wait",
+    "bf_server_get_stats",
 )
 
 BF_BATCH_FIXED_MAPPING = 1
@@ -109,6 +111,18 @@ class Tuning(C.Structure):
     _fields_ = [("lanes", (C.c_int32 * 8) * 4), ("lm_ms", ((C.c_double * 3) * 8) * 4), ("tuned", C.c_int32)]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("memory_budget", C.c_uint64), ("max_batch_fits", C.c_uint64), ("batch_flags", C.c_uint32),
+                ("max_in_flight", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("fits_completed", C.c_uint64), ("batches", C.c_uint64), ("memory_in_use", C.c_uint64),
+                ("memory_peak", C.c_uint64), ("memory_budget", C.c_uint64), ("max_batch_requests", C.c_uint64),
+                ("gpu_ms", C.c_double)]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -148,6 +162,13 @@ def load():
         lib.bf_cuda_autotune.argtypes = [vp, C.POINTER(Tuning)]
         lib.bf_cuda_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
         lib.bf_cuda_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        lib.bf_server_create.argtypes = [C.c_int, C.POINTER(ServerOptions), C.POINTER(vp)]
+        lib.bf_server_destroy.argtypes = [vp]
+        lib.bf_server_destroy.restype = None
+        lib.bf_server_submit.argtypes = [vp, C.POINTER(FitArgs), C.POINTER(FitOutputs), C.POINTER(C.c_uint64)]
+        lib.bf_server_poll.argtypes = [vp, C.c_uint64]
+        lib.bf_server_wait.argtypes = [vp, C.c_uint64, C.POINTER(C.c_double)]
+        lib.bf_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
         for name in EXPORTS:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
         _lib = lib

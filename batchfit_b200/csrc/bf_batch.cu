@@ -116,16 +116,9 @@ void default_tuning(bf_tuning &t) {
 
 int state_of(bf_cuda_context *ctx, BatchState **out) {
     if (!ctx->batch) {
-        auto *st = new BatchState();
-        default_tuning(st->tuning);
-        for (cudaEvent_t &e : st->ev) {
-            const cudaError_t err = cudaEventCreate(&e);
-            if (err != cudaSuccess) {
-                release_batch_state(st);
-                return report_cuda(err, "batch events");
-            }
-        }
-        ctx->batch = st;
+        const int rc = create_batch_state(&ctx->batch);
+        if (rc != BF_OK)
+            return rc;
     }
     *out = ctx->batch;
     return BF_OK;
@@ -369,77 +362,118 @@ cudaError_t upload(BatchState &st, Plan &plan, cudaStream_t stream) {
 
 } // namespace
 
-// Run one planned batch on the context's first stream and wait for it.
-int run_batch(bf_cuda_context *ctx, const bf_batch_segment *segments, uint32_t count, uint32_t flags) {
-    BatchState *st = nullptr;
-    int rc = state_of(ctx, &st);
-    if (rc != BF_OK)
-        return rc;
+// Plan, upload and launch one batch on `stream` with the arena and graph of `st`
+// (events st.ev[0..3] bracket it).  Returns without waiting; *launched is false
+// when the batch had no fits.  One batch per state may be in flight: the pinned
+// descriptor mirror is reused by the next call.
+int launch_planned(BatchState &st, const bf_batch_segment *segments, uint32_t count, uint32_t flags, int sms,
+                   cudaStream_t stream, bool *launched, bool *graph_used) {
+    *launched = false;
+    *graph_used = false;
     Plan plan;
-    rc = plan_batch(*st, segments, count, flags, ctx->sms, plan);
+    int rc = plan_batch(st, segments, count, flags, sms, plan);
     if (rc != BF_OK)
         return rc;
-    ctx->last = bf_cuda_timing{};
     if (plan.segs.empty())
         return BF_OK;
-    rc = reserve(*st, plan.segs.size(), size_t(plan.hdr.lm_items), plan.guess_floats);
+    rc = reserve(st, plan.segs.size(), size_t(plan.hdr.lm_items), plan.guess_floats);
     if (rc != BF_OK)
         return rc;
-    cudaStream_t stream = ctx->stream[0];
-    cudaError_t e = upload(*st, plan, stream);
+    cudaError_t e = upload(st, plan, stream);
     if (e != cudaSuccess)
         return report_cuda(e, "batch descriptors");
-    const bool use_graph = (flags & BF_BATCH_NO_GRAPH) == 0 && st->warmed;
-    e = cudaEventRecord(st->ev[0], stream);
+    const bool use_graph = (flags & BF_BATCH_NO_GRAPH) == 0 && st.warmed;
+    e = cudaEventRecord(st.ev[0], stream);
     if (e == cudaSuccess && use_graph) {
-        if (!st->graph) {
+        if (!st.graph) {
             cudaGraph_t g = nullptr;
             e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
             if (e == cudaSuccess) {
-                const cudaError_t le = launch_batch_pipeline(st->args, ctx->sms, stream, nullptr, nullptr);
+                const cudaError_t le = launch_batch_pipeline(st.args, sms, stream, nullptr, nullptr);
                 e = cudaStreamEndCapture(stream, &g);
                 if (le != cudaSuccess)
                     e = le;
             }
             if (e == cudaSuccess)
-                e = cudaGraphInstantiate(&st->graph, g, 0);
+                e = cudaGraphInstantiate(&st.graph, g, 0);
             if (g)
                 cudaGraphDestroy(g);
         }
         if (e == cudaSuccess)
-            e = cudaGraphLaunch(st->graph, stream);
-        if (e == cudaSuccess)
-            e = cudaEventRecord(st->ev[3], stream);
+            e = cudaGraphLaunch(st.graph, stream);
     } else if (e == cudaSuccess) {
-        e = launch_batch_pipeline(st->args, ctx->sms, stream, st->ev[1], st->ev[2]);
-        if (e == cudaSuccess)
-            e = cudaEventRecord(st->ev[3], stream);
-        st->warmed = e == cudaSuccess;
+        e = launch_batch_pipeline(st.args, sms, stream, st.ev[1], st.ev[2]);
+        st.warmed = st.warmed || e == cudaSuccess;
     }
     if (e == cudaSuccess)
-        e = cudaEventSynchronize(st->ev[3]);
+        e = cudaEventRecord(st.ev[3], stream);
+    if (e != cudaSuccess)
+        return report_cuda(e, "mixed batch launch");
+    *launched = true;
+    *graph_used = use_graph;
+    return BF_OK;
+}
+
+// Wait for the batch launched on `st` and report its device time.
+int finish_planned(BatchState &st, bool graph_used, bf_cuda_timing *out) {
+    cudaError_t e = cudaEventSynchronize(st.ev[3]);
     if (e == cudaSuccess)
         e = cudaGetLastError();
     if (e != cudaSuccess)
         return report_cuda(e, "mixed batch");
     float total = 0.0f;
-    cudaEventElapsedTime(&total, st->ev[0], st->ev[3]);
+    cudaEventElapsedTime(&total, st.ev[0], st.ev[3]);
     bf_cuda_timing t{};
     t.kernel_ms = total;
     t.total_ms = total;
-    t.launches = use_graph ? 1u : 5u;
+    t.launches = graph_used ? 1u : 4u;
     t.batches = 1;
-    if (!use_graph) {
+    if (!graph_used) {
         float g = 0.0f, l = 0.0f, c = 0.0f;
-        cudaEventElapsedTime(&g, st->ev[0], st->ev[1]);
-        cudaEventElapsedTime(&l, st->ev[1], st->ev[2]);
-        cudaEventElapsedTime(&c, st->ev[2], st->ev[3]);
+        cudaEventElapsedTime(&g, st.ev[0], st.ev[1]);
+        cudaEventElapsedTime(&l, st.ev[1], st.ev[2]);
+        cudaEventElapsedTime(&c, st.ev[2], st.ev[3]);
         t.guess_ms = g;
         t.lm_ms = l;
         t.covariance_ms = c;
     }
-    ctx->last = t;
+    if (out)
+        *out = t;
     return BF_OK;
+}
+
+bool planned_done(BatchState &st, cudaError_t *error) {
+    const cudaError_t e = cudaEventQuery(st.ev[3]);
+    *error = e == cudaErrorNotReady ? cudaSuccess : e;
+    return e != cudaErrorNotReady;
+}
+
+int create_batch_state(BatchState **out) {
+    auto *st = new BatchState();
+    default_tuning(st->tuning);
+    for (cudaEvent_t &e : st->ev) {
+        const cudaError_t err = cudaEventCreate(&e);
+        if (err != cudaSuccess) {
+            release_batch_state(st);
+            return report_cuda(err, "batch events");
+        }
+    }
+    *out = st;
+    return BF_OK;
+}
+
+// Run one batch on the context's first stream and wait for it.
+int run_batch(bf_cuda_context *ctx, const bf_batch_segment *segments, uint32_t count, uint32_t flags) {
+    BatchState *st = nullptr;
+    int rc = state_of(ctx, &st);
+    if (rc != BF_OK)
+        return rc;
+    ctx->last = bf_cuda_timing{};
+    bool launched = false, graph_used = false;
+    rc = launch_planned(*st, segments, count, flags, ctx->sms, ctx->stream[0], &launched, &graph_used);
+    if (rc != BF_OK || !launched)
+        return rc;
+    return finish_planned(*st, graph_used, &ctx->last);
 }
 
 bf_tuning &tuning_of(BatchState *st) { return st->tuning; }

@@ -57,6 +57,14 @@ int report_cuda(cudaError_t e, const char *what);
 int run_batch(bf_cuda_context *ctx, const bf_batch_segment *segments, uint32_t count, uint32_t flags);
 int batch_state(bf_cuda_context *ctx, BatchState **out);
 bf_tuning &tuning_of(BatchState *st);
+// A batch arena of its own (the server keeps two, one per stream).
+int create_batch_state(BatchState **out);
+int launch_planned(BatchState &st, const bf_batch_segment *segments, uint32_t count, uint32_t flags, int sms,
+                   cudaStream_t stream, bool *launched, bool *graph_used);
+int finish_planned(BatchState &st, bool graph_used, bf_cuda_timing *out);
+// True once the batch launched on `st` has completed (cudaEventQuery), false while
+// it runs; CUDA errors are returned through *error.
+bool planned_done(BatchState &st, cudaError_t *error);
 
 // Events around the kernels of one batch: guess = [start, guessed), LM =
 // [guessed, fitted), covariance = [fitted, done).

@@ -196,6 +196,49 @@ int bf_cuda_autotune(bf_cuda_context *ctx, bf_tuning *out);
 int bf_cuda_get_tuning(bf_cuda_context *ctx, bf_tuning *out);
 int bf_cuda_set_tuning(bf_cuda_context *ctx, const bf_tuning *in);
 
+/* ---- Serving: continuous batching of fit requests --------------------------
+ * No counterpart in the reference, whose submit_batch queues one batch per context
+ * and accepts no new work until it is collected (include/batchfit/metal/batch.hpp:
+ * 198-217,253-264).  A server owns one GPU, a device-memory budget and a scheduler
+ * thread.  Each request is one fit call in host memory (args->memory ==
+ * BF_MEMORY_HOST; M up to bf_cuda_batch_max_points()).  Requests are admitted in
+ * arrival order while their device buffers fit the budget, copied in, and
+ * coalesced into mixed batches (bf_cuda_fit_batch's kernels).  Up to two batches
+ * are on the GPU at once, on two streams: requests that arrive while a batch runs
+ * form the next one, which starts as soon as they are copied in and overlaps the
+ * running batch's tail.  Outputs are copied into the request's host buffers, which
+ * stay owned by the caller and must stay valid until the request completes.  A
+ * request's result is the one bf_cuda_fit_batch gives for it; batch-mates only
+ * change its lanes per fit (so results agree within the parity tolerances). */
+typedef struct bf_server bf_server;
+
+typedef struct bf_server_options {
+    uint64_t memory_budget;  /* device bytes for admitted requests; 0 = 150 GB (capped by free memory) */
+    uint64_t max_batch_fits; /* fits per launch; 0 = no limit */
+    uint32_t batch_flags;    /* BF_BATCH_* of every launch */
+    uint32_t max_in_flight;  /* batches on the GPU at once, 1 or 2; 0 = 2 */
+} bf_server_options;
+
+typedef struct bf_server_stats {
+    uint64_t submitted, completed, failed, fits_completed, batches;
+    uint64_t memory_in_use, memory_peak, memory_budget; /* bytes charged to admitted requests */
+    uint64_t max_batch_requests;                        /* most requests in one launch */
+    double gpu_ms;                                      /* summed device time of the batches */
+} bf_server_stats;
+
+int bf_server_create(int device, const bf_server_options *options, bf_server **out);
+/* Stops taking requests, completes every submitted one, then frees the server. */
+void bf_server_destroy(bf_server *server);
+/* Queues a request; *ticket identifies it.  Fails (and queues nothing) when the
+ * request is invalid or needs more device memory than the whole budget. */
+int bf_server_submit(bf_server *server, const bf_fit_args *args, const bf_fit_outputs *out, uint64_t *ticket);
+/* 1 when the request has completed, 0 while pending, -BF_ERR_INVALID_ARGUMENT for an unknown ticket. */
+int bf_server_poll(bf_server *server, uint64_t ticket);
+/* Waits for the request, releases its ticket and returns its result code;
+ * *latency_ms (optional) = submit to outputs written. */
+int bf_server_wait(bf_server *server, uint64_t ticket, double *latency_ms);
+int bf_server_get_stats(bf_server *server, bf_server_stats *out);
+
 /* A fit that allocates nothing.  No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: a host whose memory pool already owns
