@@ -442,6 +442,44 @@ int finish_planned(BatchState &st, bool graph_used, bf_cuda_timing *out) {
     return BF_OK;
 }
 
+// Size the arena for `segs` segments and `fits` fits, set the kernels up and
+// capture the graph, so that batches within those sizes neither allocate nor
+// synchronise the device.
+int prepare_planned(BatchState &st, size_t segs, size_t fits, int sms, cudaStream_t stream) {
+    int rc = reserve(st, segs, fits, fits * 8);
+    if (rc != BF_OK)
+        return rc;
+    BatchHeader empty{};
+    std::memcpy(static_cast<char *>(st.host) + st.lay.header, &empty, sizeof(empty));
+    cudaError_t e = cudaMemcpyAsync(static_cast<char *>(st.arena.ptr) + st.lay.header,
+                                    static_cast<char *>(st.host) + st.lay.header, sizeof(empty),
+                                    cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = launch_batch_pipeline(st.args, sms, stream, nullptr, nullptr);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess)
+        return report_cuda(e, "batch warm-up");
+    st.warmed = true;
+    if (!st.graph) {
+        cudaGraph_t g = nullptr;
+        e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            const cudaError_t le = launch_batch_pipeline(st.args, sms, stream, nullptr, nullptr);
+            e = cudaStreamEndCapture(stream, &g);
+            if (le != cudaSuccess)
+                e = le;
+        }
+        if (e == cudaSuccess)
+            e = cudaGraphInstantiate(&st.graph, g, 0);
+        if (g)
+            cudaGraphDestroy(g);
+        if (e != cudaSuccess)
+            return report_cuda(e, "batch graph");
+    }
+    return BF_OK;
+}
+
 bool planned_done(BatchState &st, cudaError_t *error) {
     const cudaError_t e = cudaEventQuery(st.ev[3]);
     *error = e == cudaErrorNotReady ? cudaSuccess : e;

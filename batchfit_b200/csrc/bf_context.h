@@ -62,6 +62,7 @@ int create_batch_state(BatchState **out);
 int launch_planned(BatchState &st, const bf_batch_segment *segments, uint32_t count, uint32_t flags, int sms,
                    cudaStream_t stream, bool *launched, bool *graph_used);
 int finish_planned(BatchState &st, bool graph_used, bf_cuda_timing *out);
+int prepare_planned(BatchState &st, size_t segs, size_t fits, int sms, cudaStream_t stream);
 // True once the batch launched on `st` has completed (cudaEventQuery), false while
 // it runs; CUDA errors are returned through *error.
 bool planned_done(BatchState &st, cudaError_t *error);

@@ -299,16 +299,75 @@ __device__ PeakFeature find_peak(const Group<G> &g, const Signal<MODEL> &s, cons
     return r;
 }
 
+// Extrema of the smoothed signal over blocks of 32 samples (the last block may be
+// short), for the prominence walks below, and the blocks' prefix and suffix minima
+// (bmin, bmax, pmin, smin: four arrays of ceil(M/32) floats, back to back).  Lane l
+// takes blocks l, l+G, ...
+constexpr int kWalkBlock = 32;
+template <int MODEL, int G>
+__device__ void block_extrema(const Group<G> &g, const Signal<MODEL> &s, float *bmin, float *bmax) {
+    const int blocks = (s.m + kWalkBlock - 1) / kWalkBlock;
+    for (int b = int(g.lane); b < blocks; b += G) {
+        const int first = b * kWalkBlock, end = min(s.m, first + kWalkBlock);
+        float lo = s.smooth(first), hi = lo;
+        for (int j = first + 1; j < end; ++j) {
+            const float v = s.smooth(j);
+            lo = fminf(lo, v);
+            hi = fmaxf(hi, v);
+        }
+        bmin[b] = lo;
+        bmax[b] = hi;
+    }
+    g.sync();
+    // Minima of the blocks up to b (prefix) and from b on (suffix).
+    if (g.lane == 0) {
+        float *pmin = bmax + blocks, *smin = pmin + blocks;
+        float r = bmin[0];
+        for (int b = 0; b < blocks; ++b) {
+            r = fminf(r, bmin[b]);
+            pmin[b] = r;
+        }
+        r = bmin[blocks - 1];
+        for (int b = blocks - 1; b >= 0; --b) {
+            r = fminf(r, bmin[b]);
+            smin[b] = r;
+        }
+    }
+    g.sync();
+}
+
+// A side of candidate `index` can clear the threshold only if the lowest sample
+// anywhere on that side does (walk minima are at least the side minima, and the
+// block prefix / suffix minima bound those from below): a necessary condition.
+__device__ __forceinline__ bool may_be_prominent(const float *pmin, const float *smin, int m, int index,
+                                                 float height, float threshold) {
+    if (index < 1 || index + 1 >= m)
+        return false;
+    return rsub(height, pmin[(index - 1) / kWalkBlock]) > threshold &&
+           rsub(height, smin[(index + 1) / kWalkBlock]) > threshold;
+}
+
 // detail::prominence(signal, index) > threshold (initial_guess.hpp:38-54), by one
 // lane.  The reference walks outwards on each side while the smoothed signal stays
 // at or below the start height, takes the side minima and returns height minus the
 // larger minimum.  Rounding is monotone, so that exceeds the threshold iff on both
-// sides some sample of the walk has height - sample > threshold: each walk stops
-// at its first such sample (side passes) or at the reference's stop (side fails).
-template <int MODEL> __device__ bool prominent(const Signal<MODEL> &s, int index, float threshold) {
+// sides some sample of the walk has height - sample > threshold.  Each walk stops
+// at its first such sample (side passes) or at the reference's stop (side fails),
+// and crosses whole blocks whose maximum is at most the height by their minimum.
+template <int MODEL>
+__device__ bool prominent(const Signal<MODEL> &s, const float *bmin, const float *bmax, int index,
+                          float threshold) {
     const float height = s.smooth(index);
     bool left = false;
-    for (int j = index - 1; j >= 0; --j) {
+    for (int j = index - 1; j >= 0;) {
+        if ((j & (kWalkBlock - 1)) == kWalkBlock - 1 && bmax[j / kWalkBlock] <= height) {
+            if (rsub(height, bmin[j / kWalkBlock]) > threshold) {
+                left = true;
+                break;
+            }
+            j -= kWalkBlock;
+            continue;
+        }
         const float v = s.smooth(j);
         if (v > height)
             break;
@@ -316,15 +375,23 @@ template <int MODEL> __device__ bool prominent(const Signal<MODEL> &s, int index
             left = true;
             break;
         }
+        --j;
     }
     if (!left)
         return false;
-    for (int j = index + 1; j < s.m; ++j) {
+    for (int j = index + 1; j < s.m;) {
+        if ((j & (kWalkBlock - 1)) == 0 && bmax[j / kWalkBlock] <= height) {
+            if (rsub(height, bmin[j / kWalkBlock]) > threshold)
+                return true;
+            j += kWalkBlock;
+            continue;
+        }
         const float v = s.smooth(j);
         if (v > height)
             return false;
         if (rsub(height, v) > threshold)
             return true;
+        ++j;
     }
     return false;
 }
@@ -481,6 +548,10 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         const float separation =
             smax(rmul(3.0f, xc.guess_spacing), rmul(2.0f, smin(primary.left_radius, primary.right_radius)));
         const float threshold = rmul(3.0f, noise);
+        // The edge runs are no longer needed: their buffer holds the block extrema.
+        const int blocks = (m + kWalkBlock - 1) / kWalkBlock;
+        float *bmin = scratch, *bmax = bmin + blocks, *pmin = bmax + blocks, *smin = pmin + blocks;
+        block_extrema<MODEL, G>(g, s, bmin, bmax);
         auto far_enough = [&](int j) {
             const int idx = s.raw_maximum(j);
             const int bins = idx > first ? idx - first : first - idx;
@@ -512,24 +583,78 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         auto leader = [&](float v, int j) {
             return j != m && (cut_j == m || v > cut_v || (v == cut_v && j <= cut_j));
         };
-        const bool pass1 = leader(v1, j1) && prominent(s, j1, threshold);
-        const bool pass2 = !pass1 && leader(v2, j2) && prominent(s, j2, threshold);
+        const bool pass1 = leader(v1, j1) && may_be_prominent(pmin, smin, m, j1, v1, threshold) &&
+                           prominent(s, bmin, bmax, j1, threshold);
+        const bool pass2 = !pass1 && leader(v2, j2) && may_be_prominent(pmin, smin, m, j2, v2, threshold) &&
+                           prominent(s, bmin, bmax, j2, threshold);
         float bv = pass1 ? v1 : pass2 ? v2 : 0.0f;
         int bj = pass1 ? j1 : pass2 ? j2 : m;
         argmax_pair(g, bv, bj);
         if (bj == m && cut_j != m) {
-            for (int j = 1 + int(g.lane); j + 1 < m; j += G) {
-                const float v = s.smooth_interior(j);
-                if (!(v > 0.0f && (v < cut_v || (v == cut_v && j > cut_j))))
+            // Every candidate below the cut-off, each lane its own indices.  A lane
+            // takes one step per loop turn -- a candidate check or one step of a
+            // prominence walk (the walks of prominent(), unrolled) -- so the lanes'
+            // walks run side by side instead of each turn waiting for the longest.
+            int j = 1 + int(g.lane);
+            int walk = 0; // 0: checking candidates, -1 / +1: walking left / right of j
+            int w = 0;
+            float h = 0.0f;
+            while (true) {
+                if (walk == 0) {
+                    if (j + 1 >= m)
+                        break;
+                    const float v = s.smooth_interior(j);
+                    if (v > 0.0f && (v < cut_v || (v == cut_v && j > cut_j)) && (v > bv || (v == bv && j < bj)) &&
+                        may_be_prominent(pmin, smin, m, j, v, threshold) && v > s.smooth(j - 1) &&
+                        v >= s.smooth(j + 1) && far_enough(j)) {
+                        walk = -1;
+                        w = j - 1;
+                        h = v;
+                    } else {
+                        j += G;
+                    }
                     continue;
-                if (!(v > bv || (v == bv && j < bj)))
-                    continue;
-                if (!(v > s.smooth(j - 1) && v >= s.smooth(j + 1)))
-                    continue;
-                if (!far_enough(j) || !prominent(s, j, threshold))
-                    continue;
-                bv = v;
-                bj = j;
+                }
+                bool fail = false, clear = false;
+                if (walk < 0) {
+                    if (w < 0) {
+                        fail = true;
+                    } else if ((w & (kWalkBlock - 1)) == kWalkBlock - 1 && bmax[w / kWalkBlock] <= h) {
+                        clear = rsub(h, bmin[w / kWalkBlock]) > threshold;
+                        w -= kWalkBlock;
+                    } else {
+                        const float v = s.smooth(w);
+                        fail = v > h;
+                        clear = !fail && rsub(h, v) > threshold;
+                        --w;
+                    }
+                    if (clear) { // left side clears: walk right
+                        walk = 1;
+                        w = j + 1;
+                        continue;
+                    }
+                } else {
+                    if (w >= m) {
+                        fail = true;
+                    } else if ((w & (kWalkBlock - 1)) == 0 && bmax[w / kWalkBlock] <= h) {
+                        clear = rsub(h, bmin[w / kWalkBlock]) > threshold;
+                        w += kWalkBlock;
+                    } else {
+                        const float v = s.smooth(w);
+                        fail = v > h;
+                        clear = !fail && rsub(h, v) > threshold;
+                        ++w;
+                    }
+                    if (clear) { // both sides clear: the lane's best so far
+                        bv = h;
+                        bj = j;
+                        fail = true;
+                    }
+                }
+                if (fail) {
+                    walk = 0;
+                    j += G;
+                }
             }
             argmax_pair(g, bv, bj);
         }

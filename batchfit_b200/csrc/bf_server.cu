@@ -421,6 +421,12 @@ int bf_server_create(int device, const bf_server_options *options, bf_server **o
             e = cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming);
         if (e == cudaSuccess && bf::host::create_batch_state(&slot.state) != BF_OK)
             e = cudaErrorMemoryAllocation;
+        // Arena and graph sized up front: a batch within these sizes allocates
+        // nothing and never synchronises the device.
+        const uint64_t fits = s->opt.max_batch_fits ? s->opt.max_batch_fits : (4ull << 20);
+        if (e == cudaSuccess &&
+            bf::host::prepare_planned(*slot.state, 16384, size_t(fits), s->sms, slot.stream) != BF_OK)
+            e = cudaErrorMemoryAllocation;
     }
     if (e != cudaSuccess) {
         destroy(s);

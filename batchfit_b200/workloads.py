@@ -174,3 +174,84 @@ def mixed_stream(n=65_536, seed=4, m_min=64, m_max=4096):
         x[s:s + m] = xi
         y[s:s + m] = clean + 0.01 * a * rng.normal(size=m)
     return MixedWorkload(models, counts.astype(np.int32), offsets, x, y)
+
+
+# ----------------------------------------------------------------- serving --
+SERVING_M = (64, 105, 172, 283, 463, 760, 1248, 2048)  # log-spaced over [64, 2048]
+
+
+def _mixed_rows(model, x, n, rng):
+    """n spectra of `model` on x with the mixed stream's parameter distributions."""
+    a = rng.uniform(0.5, 5.0, n)[:, None]
+    c = rng.uniform(-6.0, 6.0, n)[:, None]
+    w = np.exp(rng.uniform(np.log(0.1), np.log(3.0), n))[:, None]
+    if model == "gaussian":
+        clean = a * np.exp(-0.5 * ((x - c) / (w / 2.354820045)) ** 2)
+    elif model == "lorentzian":
+        clean = a / (1 + ((x - c) / (w / 2)) ** 2)
+    elif model == "pseudo_voigt":
+        z = (x - c) / w
+        eta = rng.uniform(0.0, 1.0, n)[:, None]
+        clean = a * ((1 - eta) * np.exp(-4 * np.log(2) * z * z) + eta / (1 + 4 * z * z))
+    else:
+        w2 = np.exp(rng.uniform(np.log(0.2), np.log(2.0), n))[:, None]
+        c2 = c + rng.uniform(0.5, 3.0, n)[:, None] * 0.5 * (w / 2 + w2)
+        a2 = a * rng.uniform(0.1, 1.0, n)[:, None]
+        clean = a / (1 + ((x - c) / (w / 2)) ** 2) + a2 / (1 + ((x - c2) / w2) ** 2)
+    return (clean + 0.01 * a * rng.normal(size=clean.shape)).astype(np.float32)
+
+
+@dataclass
+class ServingPool:
+    """Spectra for the serving stream: for every (model, M in SERVING_M) a block of
+    `rows` seeded spectra, tiled to `n_max` rows so that any request is a view."""
+
+    x: dict
+    y: dict
+    n_max: int
+
+
+def serving_pool(rows=2048, n_max=50_000, seed=5, alloc=None):
+    """``alloc(shape)`` may return pinned host arrays (default: numpy)."""
+    rng = np.random.default_rng(seed)
+    xs, ys = {}, {}
+    for model in MODEL_NAMES:
+        for m in SERVING_M:
+            x = np.linspace(-10, 10, m)
+            block = _mixed_rows(model, x, rows, rng)
+            out = alloc((n_max, m)) if alloc else np.empty((n_max, m), np.float32)
+            reps = -(-n_max // rows)
+            for r in range(reps):
+                lo = r * rows
+                hi = min(n_max, lo + rows)
+                out[lo:hi] = block[: hi - lo]
+            xs[(model, m)] = x.astype(np.float32)
+            ys[(model, m)] = out
+    return ServingPool(xs, ys, n_max)
+
+
+@dataclass
+class ServingRequest:
+    arrival: float  # seconds from the stream's start
+    model: str
+    m: int
+    n: int
+    uncertainties: bool
+
+
+def serving_stream(rate, duration, seed=5, n_max=50_000):
+    """Poisson arrivals at `rate` requests/s for `duration` s; per request N ~
+    logU[1, n_max], M ~ logU[64, 2048] (snapped to SERVING_M), a random model, half
+    with uncertainties."""
+    rng = np.random.default_rng(seed)
+    out = []
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        m_cont = np.exp(rng.uniform(np.log(64), np.log(2048)))
+        m = min(SERVING_M, key=lambda v: abs(np.log(v) - np.log(m_cont)))
+        n = int(np.exp(rng.uniform(0.0, np.log(n_max))))
+        out.append(ServingRequest(t, MODEL_NAMES[int(rng.integers(4))], m, max(1, n), bool(rng.integers(2))))
+    return out

@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--fits", type=int, default=1_000_000, help="fits per GPU per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the uneven mixed-model batch section")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream section")
     return ap.parse_args()
 
 
@@ -209,6 +211,219 @@ def accuracy_sample(w, res_np, n=20000):
             "param_err_max": s["param_err_max"], "param_err_p999": s["param_err_p999"],
             "chi2_err_max": s["chi2_err_max"], "uncertainty_status_agreement": round(us_agree, 6),
             "param_tol": 1e-4, "chi2_tol": 1e-5}, passes
+
+
+# ------------------------------------------------------- mixed and serving --
+def percentile(values, q):
+    if not values:
+        return None
+    v = sorted(values)
+    return v[min(len(v) - 1, max(0, math.ceil(q / 100.0 * len(v)) - 1))]
+
+
+def mixed_section(ctx, dev):
+    """65,536 fits of mixed models, per-fit M ~ logU[64,4096] on linspace(-10,10,M):
+    one request per (model, M) sharing its x -- what the reference's one-x-per-call
+    API takes.  Batched (one persistent launch per kernel, autotuned lanes, graph
+    replay) against the plain path: one bf_cuda_fit per request with one fit per
+    warp (32 lanes), in request order."""
+    import ctypes as C
+
+    import torch
+
+    import batchfit_b200 as bf
+    from batchfit_b200 import _capi, accuracy, workloads
+    from oracle import pyoracle
+
+    w = workloads.mixed_stream(n=65_536, seed=4)
+    groups = {}
+    for i in np.lexsort((w.counts, w.models)):
+        groups.setdefault((int(w.models[i]), int(w.counts[i])), []).append(int(i))
+    segs, keep, reqs = [], [], []
+    for (mid, m), idx in groups.items():
+        rows = np.stack([w.y[w.offsets[i]:w.offsets[i] + m] for i in idx])
+        x = w.x[w.offsets[idx[0]]:w.offsets[idx[0]] + m].copy()
+        model = workloads.MODEL_NAMES[mid]
+        lo, hi = (np.array(v, np.float32) for v in workloads.MIXED_BOUNDS[model])
+        a, o, res, k = bf._device_segment(torch.from_numpy(x).to(dev), torch.from_numpy(rows).to(dev), model,
+                                          None, (lo, hi), False, "parity", 0, None)
+        segs.append(_capi.BatchSegment(a, o))
+        keep.append((res, k))
+        reqs.append((model, x, rows, lo, hi, res))
+    arr = (_capi.BatchSegment * len(segs))(*segs)
+    lib = _capi.load()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.autotune()
+    tune_s = time.perf_counter() - t0
+    n_fits = int(w.models.size)
+
+    def batched(flags, reps=5):
+        walls, devs = [], []
+        for _ in range(2):
+            _capi.check(lib.bf_cuda_fit_batch(ctx.handle, arr, len(segs), flags), "bf_cuda_fit_batch")
+        for _ in range(reps):
+            t = time.perf_counter()
+            _capi.check(lib.bf_cuda_fit_batch(ctx.handle, arr, len(segs), flags), "bf_cuda_fit_batch")
+            walls.append(time.perf_counter() - t)
+            devs.append(ctx.timing().kernel_ms)
+        return statistics.median(walls) * 1e3, statistics.median(devs)
+
+    tuned_wall, tuned_dev = batched(0)
+    split = None
+    _capi.check(lib.bf_cuda_fit_batch(ctx.handle, arr, len(segs), _capi.BF_BATCH_NO_GRAPH), "bf_cuda_fit_batch")
+    t = ctx.timing()
+    split = {"guess_ms": round(t.guess_ms, 3), "lm_ms": round(t.lm_ms, 3), "covariance_ms": round(t.covariance_ms, 3)}
+    fixed_wall, fixed_dev = batched(_capi.BF_BATCH_FIXED_MAPPING)
+    # Results of the tuned batch for the accuracy sample.
+    _capi.check(lib.bf_cuda_fit_batch(ctx.handle, arr, len(segs), 0), "bf_cuda_fit_batch")
+    torch.cuda.synchronize()
+    sample = [(model, x, rows[:1], lo, hi, res.params[:1].cpu().numpy(), res.status[:1].cpu().numpy(),
+               res.chi2[:1].cpu().numpy()) for (model, x, rows, lo, hi, res) in reqs[::10]]
+    # Plain: one call per request, one fit per warp, device memory.
+    plain_dev = 0.0
+    t = time.perf_counter()
+    for sgm in segs:
+        a = sgm.args
+        a.group_lanes = 32
+        ctx.fit(a, sgm.out)
+        plain_dev += ctx.timing().total_ms
+        a.group_lanes = 0
+    plain_wall = (time.perf_counter() - t) * 1e3
+    # Accuracy of the batched fits on a sample (the first fit of every tenth request).
+    definite = agree = within = within32 = 0
+    for model, x, y1, lo, hi, gp, gs, gc in sample:
+        ref = pyoracle.fit("port", model, x, y1, None, lo, hi, np.float64)
+        if ref.status[0] == 1:
+            continue
+        r32 = pyoracle.fit("port", model, x, y1, None, lo, hi, np.float32)
+        s = accuracy.summarize(model, x, y1, gp, gs, gc, ref.params, ref.status, ref.chi2, 1e-4, 1e-5)
+        s32 = accuracy.summarize(model, x, y1, r32.params, r32.status, r32.chi2, ref.params, ref.status, ref.chi2,
+                                 1e-4, 1e-5)
+        definite += 1
+        agree += s["status_agreement"]
+        within += s["within_tol_fraction"]
+        within32 += s32["within_tol_fraction"]
+    del keep
+    return {
+        "workload": "mixed_stream: 65,536 fits, 25% per model, M~logU[64,4096] on linspace(-10,10,M), p0=None; "
+                    f"{len(segs)} requests (one per model and M, sharing x)",
+        "batched": {"fits_per_s": n_fits / (tuned_dev * 1e-3), "device_ms": round(tuned_dev, 3),
+                    "call_ms": round(tuned_wall, 3), "kernels_no_graph": split,
+                    "what": "autotuned lanes, one persistent launch per kernel, graph replay"},
+        "fixed_mapping": {"fits_per_s": n_fits / (fixed_dev * 1e-3), "device_ms": round(fixed_dev, 3),
+                          "call_ms": round(fixed_wall, 3), "what": "one launch, every fit on one warp, request order"},
+        "plain_per_request": {"fits_per_s": n_fits / (plain_dev * 1e-3), "device_ms": round(plain_dev, 3),
+                              "call_ms": round(plain_wall, 3),
+                              "what": "one bf_cuda_fit per request, one fit per warp (32 lanes)"},
+        "speedup_vs_plain": {"device": round(plain_dev / tuned_dev, 2), "call": round(plain_wall / tuned_wall, 2)},
+        "autotune_s": round(tune_s, 3),
+        "accuracy": {"sample_fits": len(sample), "definite": definite,
+                     "status_agreement": round(agree / max(definite, 1), 5),
+                     "within_tol_fraction": round(within / max(definite, 1), 5),
+                     "reference_float32_within_tol_fraction": round(within32 / max(definite, 1), 5),
+                     "note": "fits the float64 oracle leaves at max_iterations are excluded (no definite status)"},
+    }
+
+
+def serving_section(lib):
+    """Poisson arrivals of fit requests (N ~ logU[1,50000], M ~ logU[64,2048], random
+    model, half with uncertainties, p0=None) at several rates: the continuous-
+    batching server against plain per-request calls in arrival order (one fit per
+    warp).  Latency = arrival to outputs in host memory."""
+    import ctypes as C
+
+    import batchfit_b200 as bf
+    from batchfit_b200 import _capi, workloads
+
+    pinned = []
+
+    def alloc(shape):
+        nbytes = int(np.prod(shape)) * 4
+        ptr = C.c_void_p()
+        _capi.check(lib.bf_cuda_host_alloc(nbytes, C.byref(ptr)), "bf_cuda_host_alloc")
+        pinned.append(ptr)
+        buf = (C.c_float * int(np.prod(shape))).from_address(ptr.value)
+        return np.frombuffer(buf, np.float32).reshape(shape)
+
+    t0 = time.perf_counter()
+    pool = workloads.serving_pool(alloc=alloc)
+    pool_s = time.perf_counter() - t0
+    ctx = bf.context(0)
+    out = []
+    for k, (rate, duration) in enumerate(((10, 4.0), (100, 3.0), (1000, 2.0), (2000, 2.0))):
+        stream = workloads.serving_stream(rate, duration, seed=50 + k)
+        fits = sum(r.n for r in stream)
+
+        def views(r):
+            x = pool.x[(r.model, r.m)]
+            y = pool.y[(r.model, r.m)][:r.n]
+            lo, hi = (np.array(v, np.float32) for v in workloads.MIXED_BOUNDS[r.model])
+            return x, y, (lo, hi)
+
+        # Served.
+        with bf.Server() as server:
+            tickets = []
+            start = time.perf_counter()
+            for r in stream:
+                delay = start + r.arrival - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                x, y, bounds = views(r)
+                tickets.append(server.submit(x, y, r.model, None, bounds, uncertainties=r.uncertainties))
+            for tk in tickets:
+                tk.result()
+            end = time.perf_counter()
+            st = server.stats()
+        lat = [tk.latency_ms for tk in tickets]
+        served = {"p50_ms": round(percentile(lat, 50), 3), "p99_ms": round(percentile(lat, 99), 3),
+                  "fits_per_s": fits / (end - start), "batches": st["batches"],
+                  "max_requests_per_batch": st["max_batch_requests"], "gpu_busy_ms": round(st["gpu_ms"], 2),
+                  "memory_peak_gb": round(st["memory_peak"] / 1e9, 3)}
+        # Plain: requests served one at a time in arrival order; stops taking new
+        # requests after 6x the stream's duration (the rest are reported unserved).
+        lat_p, served_fits, unserved = [], 0, 0
+        start = time.perf_counter()
+        for r in stream:
+            now = time.perf_counter() - start
+            if now > 6 * duration + 2.0:
+                unserved += 1
+                continue
+            if r.arrival > now:
+                time.sleep(r.arrival - now)
+            x, y, bounds = views(r)
+            p = 8 if r.model == "two_lorentzian" else 4 if r.model == "pseudo_voigt" else 3
+            o = {k: np.empty(s, dt) for k, s, dt in (("params", (r.n, p), np.float32), ("status", r.n, np.int32),
+                                                     ("iters", r.n, np.uint32), ("chi2", r.n, np.float32))}
+            if r.uncertainties:
+                o.update({"cov": np.empty((r.n, p, p), np.float32), "se": np.empty((r.n, p), np.float32),
+                          "us": np.empty(r.n, np.int32)})
+            opts = bf.solver_options(r.model, bounds[0], bounds[1], "parity")
+            ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+            args = _capi.FitArgs(bf.MODELS[r.model], r.n, x.size, ptr(x), ptr(y), None, _capi.BF_MEMORY_HOST,
+                                 int(r.uncertainties), 32, opts)
+            outs = _capi.FitOutputs(ptr(o["params"]), ptr(o["status"]), ptr(o["iters"]), ptr(o["chi2"]),
+                                    ptr(o.get("cov")), ptr(o.get("se")), ptr(o.get("us")))
+            ctx.fit(args, outs)
+            done = time.perf_counter() - start
+            lat_p.append((done - r.arrival) * 1e3)
+            served_fits += r.n
+        end_p = time.perf_counter() - start
+        plain = {"p50_ms": round(percentile(lat_p, 50), 3) if lat_p else None,
+                 "p99_ms": round(percentile(lat_p, 99), 3) if lat_p else None,
+                 "fits_per_s": served_fits / end_p, "unserved_requests": unserved}
+        out.append({"rate_per_s": rate, "duration_s": duration, "requests": len(stream), "fits": fits,
+                    "served": served, "plain": plain,
+                    "p99_ratio_plain_over_served": round(plain["p99_ms"] / served["p99_ms"], 2)
+                    if plain["p99_ms"] else None,
+                    "throughput_ratio_served_over_plain": round(served["fits_per_s"] / plain["fits_per_s"], 2)})
+    for ptr in pinned:
+        lib.bf_cuda_host_free(ptr)
+    return {"stream": "Poisson arrivals; N~logU[1,50000], M~logU[64,2048] (8 log-spaced values), random model, "
+                      "half with uncertainties, p0=None; inputs in pinned host memory",
+            "pool_setup_s": round(pool_s, 2), "rates": out,
+            "plain_what": "bf_cuda_fit per request in arrival order (host buffers, one fit per warp)",
+            "served_what": "bf_server: HBM-budget admission, coalesced mixed batches, two batches in flight"}
 
 
 # -------------------------------------------------------------- arms --
@@ -388,6 +603,12 @@ def run_cuda_arm(args, world, rank, local):
     cpu = None
     if not args.no_cpu_baseline:
         cpu = cpu_reference_rate(w, args.cpu_seconds)
+    del y_d, out_d
+    torch.cuda.empty_cache()
+    # The mixed-batch and serving sections run at N=1 only (one GPU's batching and
+    # serving; the scaling runs repeat the plain workload per GPU).
+    mixed = None if args.no_mixed or world > 1 else mixed_section(ctx, dev)
+    serving = None if args.no_serving or world > 1 else serving_section(lib)
     lat = sorted(step_ms)
     line = {
         "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world, "steps": args.steps,
@@ -406,6 +627,8 @@ def run_cuda_arm(args, world, rank, local):
         "roofline": roof,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
+        "mixed": mixed,
+        "serving": serving,
         "peaks_measured": {"fp32_tflops": round(peaks.fp32_tflops, 2), "fp64_tflops": round(peaks.fp64_tflops, 2),
                            "mufu_ex2_gops": round(peaks.mufu_ex2_gops, 1),
                            "mufu_rcp_gops": round(peaks.mufu_rcp_gops, 1)},
