@@ -6,9 +6,9 @@
 //   admission  the queue's head is admitted while its device buffers fit the
 //              budget: one stream-ordered allocation from the server's memory pool,
 //              inputs copied in on the copy stream;
-//   launch     when one of the two batch slots is free, every admitted request not
-//              yet launched (up to max_batch_fits) becomes one mixed batch on that
-//              slot's stream, ordered after the copies;
+//   launch     when one of the two batch slots is free, the admitted requests whose
+//              inputs are on the device (up to max_batch_fits) become one mixed
+//              batch on that slot's stream;
 //   retire     a slot whose batch finished copies its outputs back, releases the
 //              buffers, completes its requests and returns their bytes to the budget.
 // With two slots, a batch formed while another runs starts as soon as its inputs
@@ -37,8 +37,18 @@ using Clock = std::chrono::steady_clock;
 int parameters(int model) { return model == 2 ? 4 : model == 3 ? 8 : 3; }
 size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
+// Completion of one admission round's copies on the copy stream.
+struct CopyMark {
+    cudaEvent_t event = nullptr;
+    ~CopyMark() {
+        if (event)
+            cudaEventDestroy(event);
+    }
+};
+
 struct Request {
     uint64_t ticket = 0;
+    std::shared_ptr<CopyMark> copied; // its inputs are on the device once this completes
     bf_fit_args args{};         // host pointers of the caller
     bf_fit_outputs host_out{};  // host outputs of the caller
     size_t bytes = 0;           // device bytes charged to the budget
@@ -77,7 +87,6 @@ struct bf_server {
     bf_server_options opt{};
     cudaMemPool_t pool = nullptr;
     cudaStream_t copy = nullptr;
-    cudaEvent_t copied = nullptr;
     Slot slot[2];
     std::thread worker;
     std::mutex mutex;
@@ -112,9 +121,11 @@ void complete(bf_server *s, const std::shared_ptr<Request> &r, int result) {
     s->finished.notify_all();
 }
 
-// Admit the head of the queue while it fits; returns false on a CUDA failure.
+// Admit the head of the queue while it fits: allocate its buffers and queue its
+// input copies; the round's copies share one completion mark.  False on a CUDA
+// failure.
 bool admit(bf_server *s) {
-    bool any = false;
+    std::shared_ptr<CopyMark> mark;
     while (!s->pending.empty()) {
         const std::shared_ptr<Request> &r = s->pending.front();
         {
@@ -166,12 +177,20 @@ bool admit(bf_server *s) {
             report_cuda(e, "server copy-in");
             return false;
         }
+        if (!mark) {
+            mark = std::make_shared<CopyMark>();
+            e = cudaEventCreateWithFlags(&mark->event, cudaEventDisableTiming);
+            if (e != cudaSuccess) {
+                report_cuda(e, "server copy-in event");
+                return false;
+            }
+        }
+        r->copied = mark;
         s->ready.push_back(r);
         s->pending.pop_front();
-        any = true;
     }
-    if (any) {
-        const cudaError_t e = cudaEventRecord(s->copied, s->copy);
+    if (mark) {
+        const cudaError_t e = cudaEventRecord(mark->event, s->copy);
         if (e != cudaSuccess) {
             report_cuda(e, "server copy-in event");
             return false;
@@ -182,6 +201,9 @@ bool admit(bf_server *s) {
 
 // Launch the ready requests (up to max_batch_fits) on a free slot.
 bool launch(bf_server *s, Slot &slot) {
+    // Copies complete in admission order, so the requests whose inputs are on the
+    // device are a prefix of the ready list: a batch never waits for other
+    // requests' copies.
     std::vector<std::shared_ptr<Request>> take;
     uint64_t fits = 0;
     size_t i = 0;
@@ -189,19 +211,24 @@ bool launch(bf_server *s, Slot &slot) {
         const uint64_t n = s->ready[i]->args.n;
         if (!take.empty() && s->opt.max_batch_fits && fits + n > s->opt.max_batch_fits)
             break;
+        const cudaError_t q = cudaEventQuery(s->ready[i]->copied->event);
+        if (q == cudaErrorNotReady)
+            break;
+        if (q != cudaSuccess) {
+            report_cuda(q, "server copy-in");
+            return false;
+        }
         take.push_back(s->ready[i]);
         fits += n;
     }
+    if (take.empty())
+        return true;
     s->ready.erase(s->ready.begin(), s->ready.begin() + i);
     std::vector<bf_batch_segment> segs;
     segs.reserve(take.size());
     for (auto &r : take)
         segs.push_back(r->seg);
-    cudaError_t e = cudaStreamWaitEvent(slot.stream, s->copied, 0);
-    if (e != cudaSuccess) {
-        report_cuda(e, "server stream order");
-        return false;
-    }
+    cudaError_t e = cudaSuccess;
     bool launched = false;
     const int rc = bf::host::launch_planned(*slot.state, segs.data(), uint32_t(segs.size()), s->opt.batch_flags,
                                             s->sms, slot.stream, &launched, &slot.graph_used);
@@ -312,11 +339,11 @@ void scheduler(bf_server *s) {
         {
             std::unique_lock<std::mutex> lock(s->mutex);
             const bool running = s->slot[0].busy || s->slot[1].busy;
-            const bool work = !s->incoming.empty() || !s->ready.empty() || !s->pending.empty();
-            if (!running && !work && !s->stopping)
+            const bool work = !s->ready.empty() || !s->pending.empty();
+            if (!running && !work && s->incoming.empty() && !s->stopping)
                 s->wake.wait(lock, [&] { return !s->incoming.empty() || s->stopping; });
-            else if (running && s->incoming.empty())
-                s->wake.wait_for(lock, std::chrono::microseconds(50));
+            else if (s->incoming.empty())
+                s->wake.wait_for(lock, std::chrono::microseconds(50)); // poll copies and batches
             while (!s->incoming.empty()) {
                 s->pending.push_back(std::move(s->incoming.front()));
                 s->incoming.pop_front();
@@ -355,8 +382,6 @@ void destroy(bf_server *s) {
         cudaStreamSynchronize(s->copy);
         cudaStreamDestroy(s->copy);
     }
-    if (s->copied)
-        cudaEventDestroy(s->copied);
     if (s->pool)
         cudaMemPoolDestroy(s->pool);
     delete s;
@@ -412,8 +437,17 @@ int bf_server_create(int device, const bf_server_options *options, bf_server **o
     }
     if (e == cudaSuccess)
         e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking);
-    if (e == cudaSuccess)
-        e = cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming);
+    // Map pool memory now (up to 8 GB of the budget): growing the pool while requests
+    // arrive would stall admission for milliseconds per growth.
+    if (e == cudaSuccess) {
+        void *warm = nullptr;
+        const size_t bytes = size_t(std::min<uint64_t>(budget, 8ull << 30));
+        e = cudaMallocFromPoolAsync(&warm, bytes, s->pool, s->copy);
+        if (e == cudaSuccess)
+            e = cudaFreeAsync(warm, s->copy);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s->copy);
+    }
     for (auto &slot : s->slot) {
         if (e == cudaSuccess)
             e = cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking);
