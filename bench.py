@@ -448,18 +448,18 @@ def run_reference_arm(args, world, rank):
 
     if rank != 0:
         return 0
-    n = 200_000
+    n = min(200_000, args.fits)
     w = workloads.pseudo_voigt_plain(n=n)
     from oracle import pyoracle
 
     impl = "ref" if pyoracle.ref_available() else "port"
     cores = int(pyoracle.load_ref().bfref_hardware_concurrency()) if impl == "ref" else 1
     # Size each step to a bounded sample of the workload (~1-2 s of CPU work).
-    probe = 2000
+    probe = min(2000, n)
     t0 = time.perf_counter()
     pyoracle.fit(impl, MODEL, w.x, w.y[:probe], None, w.lower, w.upper, np.float32, uncertainties=True)
     per_fit = (time.perf_counter() - t0) / probe
-    sample = int(min(n, max(probe, 1.5 / max(per_fit, 1e-9))))
+    sample = int(min(n, max(min(probe, n), 1.5 / max(per_fit, 1e-9))))
     for _ in range(args.warmup):
         pyoracle.fit(impl, MODEL, w.x, w.y[:sample], None, w.lower, w.upper, np.float32, uncertainties=True)
     times = []
