@@ -591,14 +591,22 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         int bj = pass1 ? j1 : pass2 ? j2 : m;
         argmax_pair(g, bv, bj);
         if (bj == m && cut_j != m) {
-            // Every candidate below the cut-off, each lane its own indices.  A lane
-            // takes one step per loop turn -- a candidate check or one step of a
-            // prominence walk (the walks of prominent(), unrolled) -- so the lanes'
-            // walks run side by side instead of each turn waiting for the longest.
+            // Every candidate below the cut-off, each lane its own indices (lane l
+            // takes l+1, l+1+G, ...: candidates cluster on the peaks, and interleaving
+            // spreads them over the lanes).  A lane takes one step per loop turn -- a
+            // candidate check or one step of a prominence walk (the walks of
+            // prominent(), unrolled, sliding a window over the signal: one new sample
+            // per step) -- so the lanes' walks run side by side instead of each turn
+            // waiting for the longest.
+            auto smooth3 = [](float a, float b, float c) {
+                return radd(radd(rmul(0.25f, a), rmul(0.5f, b)), rmul(0.25f, c));
+            };
             int j = 1 + int(g.lane);
+            auto advance = [&]() { j += G; };
             int walk = 0; // 0: checking candidates, -1 / +1: walking left / right of j
             int w = 0;
-            float h = 0.0f;
+            float h = 0.0f, wo = 0.0f, wi = 0.0f; // walk window: at(w), at(w -/+ 1 towards j)
+            bool fresh = true;
             while (true) {
                 if (walk == 0) {
                     if (j + 1 >= m)
@@ -610,8 +618,9 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
                         walk = -1;
                         w = j - 1;
                         h = v;
+                        fresh = true;
                     } else {
-                        j += G;
+                        advance();
                     }
                     continue;
                 }
@@ -622,15 +631,28 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
                     } else if ((w & (kWalkBlock - 1)) == kWalkBlock - 1 && bmax[w / kWalkBlock] <= h) {
                         clear = rsub(h, bmin[w / kWalkBlock]) > threshold;
                         w -= kWalkBlock;
+                        fresh = true;
                     } else {
-                        const float v = s.smooth(w);
+                        if (fresh) {
+                            wo = s.at(w);
+                            wi = s.at(w + 1);
+                            fresh = false;
+                        }
+                        float outer = 0.0f, v = wo;
+                        if (w > 0) {
+                            outer = s.at(w - 1);
+                            v = smooth3(outer, wo, wi);
+                        }
                         fail = v > h;
                         clear = !fail && rsub(h, v) > threshold;
+                        wi = wo;
+                        wo = outer;
                         --w;
                     }
                     if (clear) { // left side clears: walk right
                         walk = 1;
                         w = j + 1;
+                        fresh = true;
                         continue;
                     }
                 } else {
@@ -639,10 +661,22 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
                     } else if ((w & (kWalkBlock - 1)) == 0 && bmax[w / kWalkBlock] <= h) {
                         clear = rsub(h, bmin[w / kWalkBlock]) > threshold;
                         w += kWalkBlock;
+                        fresh = true;
                     } else {
-                        const float v = s.smooth(w);
+                        if (fresh) {
+                            wo = s.at(w);
+                            wi = s.at(w - 1);
+                            fresh = false;
+                        }
+                        float outer = 0.0f, v = wo;
+                        if (w < m - 1) {
+                            outer = s.at(w + 1);
+                            v = smooth3(wi, wo, outer);
+                        }
                         fail = v > h;
                         clear = !fail && rsub(h, v) > threshold;
+                        wi = wo;
+                        wo = outer;
                         ++w;
                     }
                     if (clear) { // both sides clear: the lane's best so far
@@ -653,7 +687,7 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
                 }
                 if (fail) {
                     walk = 0;
-                    j += G;
+                    advance();
                 }
             }
             argmax_pair(g, bv, bj);

@@ -311,3 +311,27 @@ def test_async_submit_wait(bf):
     np.testing.assert_array_equal(params, ref.params)
     t = ctx.timing()
     assert t.launches >= 1 and t.kernel_ms > 0
+
+
+def test_two_lorentzian_cube_sample_parity(bf, oracle):
+    """The overlapping-peak cube (M=1024, 5% pure-noise and 2% constant rows) on a
+    3,000-row sample, against the float64 oracle where it reaches a definite
+    status: statuses agree and parameters are within 1e-4 at least as often as the
+    reference's own float32 solver's do (this stress case is ill-conditioned: the
+    float32 reference agrees on 99.1% of statuses and 74% of parameters); rows
+    without two resolvable peaks get no guess (invalid input, as the reference)."""
+    w = W.two_lorentzian_cube(n=3000, seed=3)
+    got = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda")
+    ref = oracle.fit("port", w.model, w.x, w.y, None, w.lower, w.upper, np.float64)
+    ref32 = oracle.fit("port", w.model, w.x, w.y, None, w.lower, w.upper, np.float32)
+    definite = ref.status != 1
+    s = A.summarize(w.model, w.x, w.y[definite], got.params[definite], got.status[definite], got.chi2[definite],
+                    ref.params[definite], ref.status[definite], ref.chi2[definite], PARAM_TOL, CHI2_TOL)
+    s32 = A.summarize(w.model, w.x, w.y[definite], ref32.params[definite], ref32.status[definite],
+                      ref32.chi2[definite], ref.params[definite], ref.status[definite], ref.chi2[definite],
+                      PARAM_TOL, CHI2_TOL)
+    assert definite.mean() >= 0.95
+    assert s["status_agreement"] >= s32["status_agreement"], (s, s32)
+    assert s["within_tol_fraction"] >= s32["within_tol_fraction"], (s, s32)
+    assert np.all(got.status[w.meta["constant"]] == 3)
+    np.testing.assert_array_equal(got.status[w.meta["noise_only"]], ref.status[w.meta["noise_only"]])
