@@ -18,8 +18,17 @@
 
 namespace bf {
 
+// Guess kernel: 256 threads, 2 CTAs per SM.
 constexpr int kBlock = 256;
 constexpr int kMinBlocks = 2;
+// LM kernel CTA shape per model.  The 3- and 4-parameter passes fit in 102 registers
+// a thread: 128-thread CTAs, 5 per SM, give 20 warps per SM where 256-thread CTAs
+// fit only two (16 warps) -- measured 6-20% faster on B200.  The two-Lorentzian
+// state needs its 128 registers (it spills at 102): 256 threads, 2 per SM.
+template <int MODEL> struct LmShape {
+    static constexpr int threads = MODEL == kTwoLorentzian ? 256 : 128;
+    static constexpr int min_blocks = MODEL == kTwoLorentzian ? 2 : 5;
+};
 
 // Per-group shared memory, in 4-byte words, padded so that consecutive groups of a
 // warp start G banks apart.
@@ -35,7 +44,9 @@ __host__ __device__ inline int guess_group_words(int m, int lanes, int v) {
 }
 __host__ __device__ inline int x_words(int m) { return round_up(m, 4); }
 
-template <int MODEL, int G> int lm_smem_bytes(int m) { return 4 * (x_words(m) + (kBlock / G) * lm_group_words<MODEL>(m, G)); }
+template <int MODEL, int G> int lm_smem_bytes(int m) {
+    return 4 * (x_words(m) + (LmShape<MODEL>::threads / G) * lm_group_words<MODEL>(m, G));
+}
 template <int G, int V> int guess_smem_bytes(int m) {
     return 4 * (x_words(m) + (kBlock / G) * guess_group_words(m, G, V));
 }
@@ -126,9 +137,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) guess_kernel(const float *
 
 // --------------------------------------------------------------- LM kernel --
 template <int MODEL, int G>
-__global__ void __launch_bounds__(kBlock, kMinBlocks) lm_kernel(FitArgs a) {
+__global__ void __launch_bounds__(LmShape<MODEL>::threads, LmShape<MODEL>::min_blocks) lm_kernel(FitArgs a) {
     constexpr int P = Model<MODEL>::P;
-    constexpr int kGroups = kBlock / G;
+    constexpr int kGroups = LmShape<MODEL>::threads / G;
     extern __shared__ __align__(16) float smem[];
     __shared__ XConst xc;
     const int m = a.m;
@@ -323,13 +334,13 @@ cudaError_t measure_peaks(int sms, cudaStream_t s, PeakRates *out) {
 }
 
 // ------------------------------------------------------------ host side --
-template <class K> static cudaError_t grid_for(K kernel, int smem, long long groups_needed, int groups_per_cta,
-                                               int sms, int &grid, int &per_sm) {
+template <class K> static cudaError_t grid_for(K kernel, int block, int smem, long long groups_needed,
+                                               int groups_per_cta, int sms, int &grid, int &per_sm) {
     cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void *>(kernel),
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess)
         return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem);
     if (e != cudaSuccess)
         return e;
     if (per_sm < 1)
@@ -347,12 +358,13 @@ static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t strea
                                    cudaEvent_t lm_done) {
     const int smem = lm_smem_bytes<MODEL, G>(a.m);
     int grid = 0, per_sm = 0;
-    cudaError_t e = grid_for(lm_kernel<MODEL, G>, smem, a.n, kBlock / G, sms, grid, per_sm);
+    constexpr int kThreads = LmShape<MODEL>::threads;
+    cudaError_t e = grid_for(lm_kernel<MODEL, G>, kThreads, smem, a.n, kThreads / G, sms, grid, per_sm);
     if (e != cudaSuccess)
         return e;
-    lm_kernel<MODEL, G><<<grid, kBlock, smem, stream>>>(a);
+    lm_kernel<MODEL, G><<<grid, kThreads, smem, stream>>>(a);
     if (info)
-        *info = LaunchInfo{grid, kBlock, smem, per_sm, G};
+        *info = LaunchInfo{grid, kThreads, smem, per_sm, G};
     e = cudaGetLastError();
     if (e == cudaSuccess && lm_done)
         e = cudaEventRecord(lm_done, stream);
@@ -367,7 +379,7 @@ static cudaError_t launch_guess_typed(const float *x, const float *y, long long 
                                       int32_t *status, int sms, cudaStream_t stream) {
     const int smem = guess_smem_bytes<G, V>(m);
     int grid = 0, per_sm = 0;
-    cudaError_t e = grid_for(guess_kernel<MODEL, G, V>, smem, n, kBlock / G, sms, grid, per_sm);
+    cudaError_t e = grid_for(guess_kernel<MODEL, G, V>, kBlock, smem, n, kBlock / G, sms, grid, per_sm);
     if (e != cudaSuccess)
         return e;
     guess_kernel<MODEL, G, V><<<grid, kBlock, smem, stream>>>(x, y, n, m, guesses, status);
