@@ -18,9 +18,13 @@
 
 namespace bf {
 
-// Guess kernel: 256 threads, 2 CTAs per SM.
-constexpr int kBlock = 256;
-constexpr int kMinBlocks = 2;
+// Guess kernel CTA shape per register-sort width V: up to 8 values per lane the
+// guess fits in 96 registers, so 128-thread CTAs, 5 per SM (20 warps); wider sorts
+// need 128 registers: 256 threads, 2 per SM.
+template <int V> struct GuessShapeCfg {
+    static constexpr int threads = V > 0 && V <= 8 ? 128 : 256;
+    static constexpr int min_blocks = V > 0 && V <= 8 ? 5 : 2;
+};
 // LM kernel CTA shape per model.  The 3- and 4-parameter passes fit in 102 registers
 // a thread: 128-thread CTAs, 5 per SM, give 20 warps per SM where 256-thread CTAs
 // fit only two (16 warps) -- measured 6-20% faster on B200.  The two-Lorentzian
@@ -48,7 +52,7 @@ template <int MODEL, int G> int lm_smem_bytes(int m) {
     return 4 * (x_words(m) + (LmShape<MODEL>::threads / G) * lm_group_words<MODEL>(m, G));
 }
 template <int G, int V> int guess_smem_bytes(int m) {
-    return 4 * (x_words(m) + (kBlock / G) * guess_group_words(m, G, V));
+    return 4 * (x_words(m) + (GuessShapeCfg<V>::threads / G) * guess_group_words(m, G, V));
 }
 
 // CTA prologue: stage x and derive the grid constants (solver.hpp:58-69,223-239;
@@ -105,10 +109,10 @@ __device__ void cta_prologue(const float *x, int m, float *xs, XConst &xc) {
 // G lanes per spectrum; V edge values per lane sorted in registers (V == 0: the
 // shared-memory sorting path for very long spectra).
 template <int MODEL, int G, int V>
-__global__ void __launch_bounds__(kBlock, kMinBlocks) guess_kernel(const float *x, const float *y, long long n,
+__global__ void __launch_bounds__(GuessShapeCfg<V>::threads, GuessShapeCfg<V>::min_blocks) guess_kernel(const float *x, const float *y, long long n,
                                                                    int m, float *guesses, int32_t *guess_status) {
     constexpr int P = Model<MODEL>::P;
-    constexpr int kGroups = kBlock / G;
+    constexpr int kGroups = GuessShapeCfg<V>::threads / G;
     extern __shared__ __align__(16) float smem[];
     __shared__ XConst xc;
     float *xs = smem;
@@ -379,10 +383,11 @@ static cudaError_t launch_guess_typed(const float *x, const float *y, long long 
                                       int32_t *status, int sms, cudaStream_t stream) {
     const int smem = guess_smem_bytes<G, V>(m);
     int grid = 0, per_sm = 0;
-    cudaError_t e = grid_for(guess_kernel<MODEL, G, V>, kBlock, smem, n, kBlock / G, sms, grid, per_sm);
+    constexpr int kThreads = GuessShapeCfg<V>::threads;
+    cudaError_t e = grid_for(guess_kernel<MODEL, G, V>, kThreads, smem, n, kThreads / G, sms, grid, per_sm);
     if (e != cudaSuccess)
         return e;
-    guess_kernel<MODEL, G, V><<<grid, kBlock, smem, stream>>>(x, y, n, m, guesses, status);
+    guess_kernel<MODEL, G, V><<<grid, kThreads, smem, stream>>>(x, y, n, m, guesses, status);
     return cudaGetLastError();
 }
 
