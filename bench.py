@@ -40,10 +40,10 @@ MODEL, M, P = "pseudo_voigt", 512, 4
 WORKLOAD = "pseudo_voigt_plain: 1M pseudo-Voigt fits, M=512, float32, p0=None, uncertainties=True"
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) of the LM kernel per fit, from the committed ncu capture
-# of the same kernel on 100,000 fits (profiles/fit_kernels_pv512_100k.md): 206.49 MB
-# read + 5.81 MB written.  Traffic grows with the fits processed, so the bench scales
+# of the same kernel on 100,000 fits (profiles/fit_kernels_pv512_100k.md): 206.54 MB
+# read + 5.55 MB written.  Traffic grows with the fits processed, so the bench scales
 # it to the launch's fit count.
-TRAFFIC_BYTES_PER_FIT = (206.486784e6 + 5.806336e6) / 100_000
+TRAFFIC_BYTES_PER_FIT = (206.537216e6 + 5.547520e6) / 100_000
 
 
 def parse():
@@ -153,12 +153,23 @@ class ClockSampler:
                 "samples": len(sms)}
 
 
+HBM_FALLBACK_GBS = 6650.0  # an earlier copy-bandwidth measurement on this pool's B200s
+
+
 def measured_peaks():
     try:
         with open(PEAKS_PATH) as f:
             return json.load(f)
     except (OSError, ValueError):
         return {}
+
+
+def hbm_peak():
+    """(GB/s, source): MEASURED_PEAKS.json's hbm_gbs, else the fallback."""
+    hbm_gbs_peak, hbm_source = hbm_peak()
+    if mp.get("hbm_gbs"):
+        return float(mp["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    return HBM_FALLBACK_GBS, "fallback 6650 GB/s (MEASURED_PEAKS.json absent; of fallback)"
 
 
 # ------------------------------------------------------------- CPU legs --
@@ -592,7 +603,7 @@ def run_cuda_arm(args, world, rank, local):
     mufu_rate = mufu * n / (k_ms * 1e-3) / 1e9
     mufu_peak = min(peaks.mufu_ex2_gops, peaks.mufu_rcp_gops)
     ideal_ms = max(flops * n / (peaks.fp32_tflops * 1e12), mufu * n / (mufu_peak * 1e9),
-                   roofline.observation_bytes(M, P, True) * n / (measured_peaks().get("hbm_gbs", 6650.0) * 1e9)) * 1e3
+                   roofline.observation_bytes(M, P, True) * n / (hbm_peak()[0] * 1e9)) * 1e3
     hbm_gbs = roofline.observation_bytes(M, P, True) * n / (all_ms * 1e-3) / 1e9
     guess_gbs = 4 * M * n / (g_ms * 1e-3) / 1e9
     mp = measured_peaks()
@@ -606,13 +617,12 @@ def run_cuda_arm(args, world, rank, local):
         "kernels_ms": {"guess": round(g_ms, 4), "lm": round(k_ms, 4),
                        "covariance": round(statistics.mean(split["covariance_ms"]), 4)},
         "guess_hbm": {"achieved": round(guess_gbs, 1), "unit": "GB/s",
-                      "frac": round(guess_gbs / mp["hbm_gbs"], 4) if mp.get("hbm_gbs") else None,
-                      "what": "y bytes read by the guess kernel / its duration, of measured hbm_gbs"},
+                      "frac": round(guess_gbs / hbm_gbs_peak, 4), "peak_source": hbm_source,
+                      "what": "y bytes read by the guess kernel / its duration"},
         "mufu": {"achieved_gops": round(mufu_rate, 1), "peak_gops": round(mufu_peak, 1),
                  "frac": round(mufu_rate / mufu_peak, 4)},
-        "hbm": {"achieved": round(hbm_gbs, 1), "peak": mp.get("hbm_gbs"), "unit": "GB/s",
-                "frac": round(hbm_gbs / mp["hbm_gbs"], 4) if mp.get("hbm_gbs") else None,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+        "hbm": {"achieved": round(hbm_gbs, 1), "peak": hbm_gbs_peak, "unit": "GB/s",
+                "frac": round(hbm_gbs / hbm_gbs_peak, 4), "peak_source": hbm_source,
                 "what": "observation bytes of the whole fit / all kernels' duration"},
         "work": {"flops_per_fit": round(flops), "mufu_per_fit": round(mufu), "oracle_passes": passes},
     }
