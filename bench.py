@@ -166,7 +166,7 @@ def measured_peaks():
 
 def hbm_peak():
     """(GB/s, source): MEASURED_PEAKS.json's hbm_gbs, else the fallback."""
-    hbm_gbs_peak, hbm_source = hbm_peak()
+    mp = measured_peaks()
     if mp.get("hbm_gbs"):
         return float(mp["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
     return HBM_FALLBACK_GBS, "fallback 6650 GB/s (MEASURED_PEAKS.json absent; of fallback)"
@@ -606,7 +606,7 @@ def run_cuda_arm(args, world, rank, local):
                    roofline.observation_bytes(M, P, True) * n / (hbm_peak()[0] * 1e9)) * 1e3
     hbm_gbs = roofline.observation_bytes(M, P, True) * n / (all_ms * 1e-3) / 1e9
     guess_gbs = 4 * M * n / (g_ms * 1e-3) / 1e9
-    mp = measured_peaks()
+    hbm_gbs_peak, hbm_source = hbm_peak()
     roof = {
         "bound": "fp32", "kernel": "lm_kernel<pseudo_voigt, 8 lanes>", "achieved": round(achieved_tf, 3),
         "peak": round(peaks.fp32_tflops, 3), "unit": "TFLOP/s", "frac": round(achieved_tf / peaks.fp32_tflops, 4),
