@@ -2,12 +2,14 @@
 // the lanes-per-fit autotuner (include/batchfit_cuda.h, "Mixed batches").
 //
 // Planner.  Every segment (one fit call) becomes one LM run, filed under the class
-// (model, lanes per fit, octave of M), and, when it has no p0, one guess run under
-// (model, guess lanes, register width, octave of M).  Classes are ordered by their
-// costliest fit (M x LM state size), largest first, and runs within a class by M,
-// largest first: the persistent kernels then finish on the cheapest fits.  The
-// fixed mapping (the plain baseline) files every fit of a model under one 32-lane
-// class and keeps the call order.
+// (model, lanes per fit, octave of M when several fits share a warp), and, when it
+// has no p0, one guess run under (model, guess lanes, register width).  Classes are
+// ordered by their costliest fit (M x LM state size), largest first, and runs
+// within a class by M, largest first: the persistent kernels then finish on the
+// cheapest fits.  Few, large classes matter: warps of one SM that run different
+// classes run different template instantiations, which thrashes the instruction
+// cache.  The fixed mapping (the plain baseline) files every fit of a model under
+// one 32-lane class and keeps the call order.
 //
 // Arena.  One device allocation holds the batch header, segments, classes, runs,
 // work items, class counters and the guess buffers.  Its layout depends only on
@@ -271,8 +273,9 @@ int plan_batch(BatchState &st, const bf_batch_segment *segments, uint32_t count,
         tuned_width.push_back(lanes == 0 && !fixed);
         if (lanes == 0)
             lanes = fixed ? 32 : st.tuning.lanes[args.model][bucket_of(args.m)];
-        // Fits of one class share a warp's code path; a class spans M within a factor
-        // of two so that the groups of a warp run passes of similar length.
+        // Fits of one class share a warp's code path; a class of several fits per warp
+        // spans M within a factor of two, so that its groups run passes of similar
+        // length.
         const int octave = fixed ? 0 : 31 - __builtin_clz(args.m);
         lm_keys.emplace_back(args.model, lanes, 0, octave);
         lm_cost.push_back(double(args.m) * state_size(args.model));
@@ -281,7 +284,8 @@ int plan_batch(BatchState &st, const bf_batch_segment *segments, uint32_t count,
         if (!args.p0) {
             int gl = 0, gv = 0;
             batch_guess_shape(int(args.m), &gl, &gv);
-            guess_keys.emplace_back(args.model, gl, gv, 31 - __builtin_clz(args.m));
+            // The shape bounds M to a factor of four within a guess class.
+            guess_keys.emplace_back(args.model, gl, gv, 0);
             guess_cost.push_back(double(args.m));
             guess_m.push_back(args.m);
             plan.guess_runs.push_back(WorkRun{s, 0, 0, (long long)args.n, 0});
@@ -307,6 +311,10 @@ int plan_batch(BatchState &st, const bf_batch_segment *segments, uint32_t count,
             if (tuned_width[r] && lanes < 32 && fits[lm_keys[r]] < 4 * slots)
                 std::get<1>(lm_keys[r]) = 32;
         }
+        // One fit per warp needs no split by M: 32-lane classes merge per model.
+        for (auto &k : lm_keys)
+            if (std::get<1>(k) == 32)
+                std::get<3>(k) = 0;
     }
     order_runs(plan.lm_runs, lm_keys, lm_cost, lm_m, fixed, plan.lm_classes);
     order_runs(plan.guess_runs, guess_keys, guess_cost, guess_m, fixed, plan.guess_classes);
