@@ -25,7 +25,7 @@ import numpy as np
 from . import _capi
 
 __version__ = "0.1.0"
-__all__ = ["fit", "fit_batch", "autotune", "Server", "FitResult", "FitResultWithUncertainties", "FitStatus",
+__all__ = ["fit", "fit_batch", "fit_npy", "autotune", "Server", "FitResult", "FitResultWithUncertainties", "FitStatus",
            "UncertaintyStatus", "cuda_available", "MODELS", "__version__"]
 
 MODELS = {"gaussian": 0, "lorentzian": 1, "pseudo_voigt": 2, "two_lorentzian": 3}
@@ -431,3 +431,10 @@ def guess(x, y, model="lorentzian"):
     ptr = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
     context(0).guess(MODELS[model], n, x.size, ptr(x), ptr(y), _capi.BF_MEMORY_HOST, ptr(params), ptr(status))
     return params, status
+
+
+def fit_npy(*args, **kwargs):
+    """Out-of-core fits from .npy files; see ``batchfit_b200.npy.fit_npy``."""
+    from .npy import fit_npy as _fit_npy
+
+    return _fit_npy(*args, **kwargs)

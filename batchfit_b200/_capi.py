@@ -32,7 +32,7 @@ EXPORTS = (
     "bf_cuda_max_points", "bf_cuda_measure_peaks", "bf_cuda_fit_noalloc", "bf_cuda_fit_batch",
     "bf_cuda_batch_max_points", "bf_cuda_autotune", "bf_cuda_get_tuning", "bf_cuda_set_tuning",
     "bf_server_create", "bf_server_destroy", "bf_server_submit", "bf_server_poll", "bf_server_wait",
-    "bf_server_get_stats",
+    "bf_server_get_stats", "bf_cuda_fit_npy", "bf_npy_inspect",
 )
 
 BF_BATCH_FIXED_MAPPING = 1
@@ -123,6 +123,17 @@ class ServerStats(C.Structure):
                 ("gpu_ms", C.c_double)]
 
 
+class NpyOptions(C.Structure):
+    _fields_ = [("model", C.c_int32), ("uncertainties", C.c_int32), ("chunk_fits", C.c_uint64),
+                ("in_flight", C.c_uint32), ("solver", SolverOptions)]
+
+
+class NpyStats(C.Structure):
+    _fields_ = [("fits", C.c_uint64), ("chunks", C.c_uint64), ("chunk_fits", C.c_uint64),
+                ("wall_seconds", C.c_double), ("read_seconds", C.c_double), ("fit_seconds", C.c_double),
+                ("write_seconds", C.c_double)]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -169,6 +180,10 @@ def load():
         lib.bf_server_poll.argtypes = [vp, C.c_uint64]
         lib.bf_server_wait.argtypes = [vp, C.c_uint64, C.POINTER(C.c_double)]
         lib.bf_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
+        lib.bf_cuda_fit_npy.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(NpyOptions),
+                                        C.POINTER(NpyStats)]
+        lib.bf_npy_inspect.argtypes = [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_uint64)]
         for name in EXPORTS:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
         _lib = lib

@@ -239,6 +239,33 @@ int bf_server_poll(bf_server *server, uint64_t ticket);
 int bf_server_wait(bf_server *server, uint64_t ticket, double *latency_ms);
 int bf_server_get_stats(bf_server *server, bf_server_stats *out);
 
+/* ---- NPY streaming -----------------------------------------------------------
+ * Out-of-core fits straight from .npy files: the reference's metal::fit_npy
+ * (include/batchfit/metal/pipeline.hpp:49-67) behind its batchfit_fit_npy tool
+ * (tools/fit_npy.cpp:20-121).  x_path holds x[M], y_path y[N,M] (fit-major, read
+ * in chunks, never whole), initial_path (or NULL for data-only guesses) p0[N,P];
+ * float32 or float64 (converted to float32), C order.  output_dir must not exist;
+ * it receives parameters.npy (<f4 [N,P]), chi_squared.npy (<f4 [N]), status.npy
+ * and iterations.npy (<u4 [N]) as the reference tool writes them, plus
+ * covariance.npy, standard_errors.npy and uncertainty_status.npy with
+ * uncertainties.  On failure the directory is removed. */
+typedef struct bf_npy_options {
+    int32_t model;           /* BF_MODEL_* */
+    int32_t uncertainties;
+    uint64_t chunk_fits;     /* fits per chunk; 0 = about 128 MB of y */
+    uint32_t in_flight;      /* pinned chunks being read or fitted at once, 1..3; 0 = 3 */
+    bf_solver_options solver;
+} bf_npy_options;
+typedef struct bf_npy_stats {
+    uint64_t fits, chunks, chunk_fits;
+    double wall_seconds, read_seconds, fit_seconds, write_seconds;
+} bf_npy_stats;
+int bf_cuda_fit_npy(bf_cuda_context *ctx, const char *x_path, const char *y_path, const char *initial_path,
+                    const char *output_dir, const bf_npy_options *options, bf_npy_stats *stats);
+/* Header of an .npy file: dtype 0 <f4, 1 <f8, 2 <u4; rank 1 or 2; shape[1] = 0 for
+ * rank 1 (npy::inspect, src/cpu/npy.cpp:88-91).  Host only: needs no GPU. */
+int bf_npy_inspect(const char *path, int32_t *dtype, int32_t *rank, uint64_t *shape);
+
 /* A fit that allocates nothing.  No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: a host whose memory pool already owns

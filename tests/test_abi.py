@@ -15,7 +15,7 @@ HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
 
 def declared_entry_points():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"\b(bf_(?:cuda|server)_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(bf_(?:cuda|server|npy)_\w+)\s*\(", text)))
 
 
 def test_header_declares_the_binding_table():
