@@ -25,7 +25,7 @@ import numpy as np
 from . import _capi
 
 __version__ = "0.1.0"
-__all__ = ["fit", "fit_batch", "fit_npy", "autotune", "Server", "FitResult", "FitResultWithUncertainties", "FitStatus",
+__all__ = ["fit", "fit_batch", "fit_npy", "fit_physical", "autotune", "Server", "FitResult", "FitResultWithUncertainties", "FitStatus",
            "UncertaintyStatus", "cuda_available", "MODELS", "__version__"]
 
 MODELS = {"gaussian": 0, "lorentzian": 1, "pseudo_voigt": 2, "two_lorentzian": 3}
@@ -438,3 +438,59 @@ def fit_npy(*args, **kwargs):
     from .npy import fit_npy as _fit_npy
 
     return _fit_npy(*args, **kwargs)
+
+
+def fit_physical(x, y, model="lorentzian", p0=None, bounds=None, *, uncertainties=False, policy="parity",
+                 group_lanes=0, options=None):
+    """Fit float64 data in normalised coordinates, results in physical units.
+
+    The reference's ``Coordinates`` recipe (include/batchfit/coordinates.hpp):
+    x is centred and scaled by its half range, each spectrum by its largest |y|,
+    in double on the GPU; the fit runs in float32 on the normalised data and
+    parameters, chi2, covariance and standard errors come back in physical units
+    as float64 numpy arrays.  ``p0`` is in physical units; ``bounds`` are in
+    fitted (normalised) units, as the reference requires.
+    """
+    import torch
+
+    if model not in _PARAMETERS:
+        raise ValueError(f"unknown model {model!r}; choose one of {tuple(_PARAMETERS)}")
+    x = np.ascontiguousarray(_real_array(x, "x"), dtype=np.float64)
+    y = np.ascontiguousarray(_real_array(y, "y"), dtype=np.float64)
+    if y.ndim == 1:
+        y = y.reshape(1, -1)
+    if x.ndim != 1 or not x.size or y.ndim != 2 or y.shape[1] != x.size:
+        raise ValueError("expected x[M] and y[N,M] with M>0")
+    n, p = y.shape[0], _PARAMETERS[model]
+    if p0 is not None:
+        p0 = np.asarray(_real_array(p0, "p0"), dtype=np.float64)
+        if p0.shape == (p,):
+            p0 = np.broadcast_to(p0, (n, p))
+        if p0.shape != (n, p):
+            raise ValueError(f"p0 must have shape [{p}] or [{n},{p}]")
+        p0 = np.ascontiguousarray(p0)
+    lower, upper = _bounds(bounds, p)
+    opts = options if options is not None else solver_options(model, lower, upper, policy)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    xd, yd = torch.from_numpy(x).to(dev), torch.from_numpy(y).to(dev)
+    pd = None if p0 is None else torch.from_numpy(p0).to(dev)
+    kw = dict(device=dev)
+    params = torch.empty((n, p), dtype=torch.float64, **kw)
+    status = torch.empty(n, dtype=torch.int32, **kw)
+    iterations = torch.empty(n, dtype=torch.int32, **kw)
+    chi2 = torch.empty(n, dtype=torch.float64, **kw)
+    cov = torch.empty((n, p, p), dtype=torch.float64, **kw) if uncertainties else None
+    se = torch.empty((n, p), dtype=torch.float64, **kw) if uncertainties else None
+    us = torch.empty(n, dtype=torch.int32, **kw) if uncertainties else None
+    ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())  # noqa: E731
+    args = _capi.PhysicalArgs(MODELS[model], n, x.size, ptr(xd), ptr(yd), ptr(pd), int(bool(uncertainties)),
+                              int(group_lanes), opts)
+    outs = _capi.PhysicalOutputs(ptr(params), ptr(status), ptr(iterations), ptr(chi2), ptr(cov), ptr(se), ptr(us))
+    torch.cuda.current_stream(dev).synchronize()
+    ctx = context(dev.index or 0)
+    _capi.check(ctx._lib.bf_cuda_fit_physical(ctx.handle, C.byref(args), C.byref(outs)), "bf_cuda_fit_physical")
+    np_ = lambda t: None if t is None else t.cpu().numpy()  # noqa: E731
+    if uncertainties:
+        return FitResultWithUncertainties(np_(params), np_(status), np_(iterations).astype(np.uint32), np_(chi2),
+                                          np_(cov), np_(se), np_(us))
+    return FitResult(np_(params), np_(status), np_(iterations).astype(np.uint32), np_(chi2))

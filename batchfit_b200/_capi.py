@@ -32,7 +32,7 @@ EXPORTS = (
     "bf_cuda_max_points", "bf_cuda_measure_peaks", "bf_cuda_fit_noalloc", "bf_cuda_fit_batch",
     "bf_cuda_batch_max_points", "bf_cuda_autotune", "bf_cuda_get_tuning", "bf_cuda_set_tuning",
     "bf_server_create", "bf_server_destroy", "bf_server_submit", "bf_server_poll", "bf_server_wait",
-    "bf_server_get_stats", "bf_cuda_fit_npy", "bf_npy_inspect",
+    "bf_server_get_stats", "bf_cuda_fit_npy", "bf_npy_inspect", "bf_cuda_fit_physical",
 )
 
 BF_BATCH_FIXED_MAPPING = 1
@@ -134,6 +134,17 @@ class NpyStats(C.Structure):
                 ("write_seconds", C.c_double)]
 
 
+class PhysicalArgs(C.Structure):
+    _fields_ = [("model", C.c_int32), ("n", C.c_uint64), ("m", C.c_uint32), ("x", C.c_void_p), ("y", C.c_void_p),
+                ("p0", C.c_void_p), ("uncertainties", C.c_int32), ("group_lanes", C.c_int32),
+                ("options", SolverOptions)]
+
+
+class PhysicalOutputs(C.Structure):
+    _fields_ = [("params", C.c_void_p), ("status", C.c_void_p), ("iterations", C.c_void_p), ("chi2", C.c_void_p),
+                ("covariance", C.c_void_p), ("standard_errors", C.c_void_p), ("uncertainty_status", C.c_void_p)]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -182,6 +193,7 @@ def load():
         lib.bf_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
         lib.bf_cuda_fit_npy.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(NpyOptions),
                                         C.POINTER(NpyStats)]
+        lib.bf_cuda_fit_physical.argtypes = [vp, C.POINTER(PhysicalArgs), C.POINTER(PhysicalOutputs)]
         lib.bf_npy_inspect.argtypes = [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                        C.POINTER(C.c_uint64)]
         for name in EXPORTS:

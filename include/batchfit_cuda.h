@@ -266,6 +266,40 @@ int bf_cuda_fit_npy(bf_cuda_context *ctx, const char *x_path, const char *y_path
  * rank 1 (npy::inspect, src/cpu/npy.cpp:88-91).  Host only: needs no GPU. */
 int bf_npy_inspect(const char *path, int32_t *dtype, int32_t *rank, uint64_t *shape);
 
+/* ---- Physical units -----------------------------------------------------------
+ * Fits of float64 data in normalised coordinates: the reference's struct
+ * Coordinates (include/batchfit/coordinates.hpp:15-113).  Per call, x is centred on
+ * the midpoint of its range and scaled by the half range; per fit, y is scaled by
+ * its largest |y| (1 when all zero); both in double, then rounded to float32 for
+ * the fit.  p0 (physical units, or NULL for data-only guesses on the normalised
+ * data) is normalised the same way.  Bounds in `options` are in fitted
+ * (normalised) units, as the reference requires.  Outputs come back in physical
+ * units in double: parameters, chi-squared (x y_scale^2), covariance (T C T^T with
+ * the reference's transform) and standard errors (square roots of its diagonal,
+ * NaN without a covariance).  Non-finite inputs or a zero x range are refused
+ * with BF_ERR_INVALID_ARGUMENT.  Device memory only. */
+typedef struct bf_physical_args {
+    int32_t model;
+    uint64_t n;
+    uint32_t m;
+    const double *x;  /* [M] */
+    const double *y;  /* [N*M] fit-major */
+    const double *p0; /* [N*P] physical units, or NULL */
+    int32_t uncertainties;
+    int32_t group_lanes; /* 0 = tuned choice */
+    bf_solver_options options;
+} bf_physical_args;
+typedef struct bf_physical_outputs {
+    double *params;             /* [N*P] physical units */
+    int32_t *status;            /* [N] */
+    uint32_t *iterations;       /* [N] */
+    double *chi2;               /* [N] physical units */
+    double *covariance;         /* [N*P*P] when uncertainties */
+    double *standard_errors;    /* [N*P] when uncertainties */
+    int32_t *uncertainty_status;/* [N] when uncertainties */
+} bf_physical_outputs;
+int bf_cuda_fit_physical(bf_cuda_context *ctx, const bf_physical_args *args, const bf_physical_outputs *out);
+
 /* A fit that allocates nothing.  No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: a host whose memory pool already owns
