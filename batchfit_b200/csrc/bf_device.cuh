@@ -120,6 +120,12 @@ __host__ __device__ constexpr int pow2ceil(int v) {
     return p;
 }
 
+// Slots of a reduce-scatter of v sums over G lanes: a multiple of G when v >= G
+// (every level halves a lane's slots), else a power of two dividing G (replicated
+// owners).  Padding slots are zeros; the butterfly pairs the same lanes in the same
+// order whatever the padding, so the reduced values do not depend on it.
+__host__ __device__ constexpr int reduce_slots(int v, int g) { return v >= g ? (v + g - 1) / g * g : pow2ceil(v); }
+
 // Reduce-scatter of KP per-lane partial sums over the G lanes of a group with a
 // two-sum at every tree level.  At each level a lane keeps half of its live slots
 // and ships the other half to its partner, so the shuffle count is ~KP instead of

@@ -70,9 +70,9 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
     using L = Layout<MODEL>;
     constexpr int P = L::P;
     constexpr int KC = P + 1;                 // chi2 and J^T r
-    constexpr int KCP = pow2ceil(KC);
+    constexpr int KCP = reduce_slots(KC, G);
     constexpr int T = P * (P + 1) / 2;        // J^T J lower triangle
-    constexpr int TP = pow2ceil(T);
+    constexpr int TP = reduce_slots(T, G);
     const auto q = Model<MODEL>::prepare(p);
     float hi[KCP], lo[KCP], aa[TP];
 #pragma unroll
