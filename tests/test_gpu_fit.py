@@ -335,3 +335,39 @@ def test_two_lorentzian_cube_sample_parity(bf, oracle):
     assert s["within_tol_fraction"] >= s32["within_tol_fraction"], (s, s32)
     assert np.all(got.status[w.meta["constant"]] == 3)
     np.testing.assert_array_equal(got.status[w.meta["noise_only"]], ref.status[w.meta["noise_only"]])
+
+
+@pytest.mark.parametrize("model", ["gaussian", "lorentzian", "pseudo_voigt", "two_lorentzian"])
+def test_largest_supported_m(bf, oracle, model):
+    """The largest M the shared-memory kernels take (groups widen to whole warps):
+    parity with the float64 oracle holds there, and one point more is refused."""
+    m = int(bf._capi.load().bf_cuda_max_points(bf.MODELS[model]))
+    x, y, lo, hi = synthetic(model, 24, m, seed=11 + m)
+    got = bf.fit(x, y, model, None, (lo, hi), "cuda")
+    ref = oracle.fit("port", model, x, y, None, lo, hi, np.float64)
+    s = A.summarize(model, x, y, got.params, got.status, got.chi2, ref.params, ref.status, ref.chi2, PARAM_TOL,
+                    CHI2_TOL)
+    assert s["status_agreement"] >= 23 / 24 and s["within_tol_fraction"] >= 22 / 24, s
+    x2 = np.linspace(-10, 10, m + 1).astype(np.float32)
+    with pytest.raises(ValueError, match="exceeds"):
+        bf.fit(x2, np.zeros((1, m + 1), np.float32), model, None, (lo, hi), "cuda")
+
+
+@pytest.mark.parametrize("m", [1, 2, 4, 5, 6])
+def test_tiny_spectra_match_the_oracle(bf, oracle, m):
+    """Spectra too short for a guess (M < 5) get the reference's invalid-input
+    status; M = 5, 6 fit like the reference (statuses equal, given p0 too)."""
+    rng = np.random.default_rng(m)
+    x = np.linspace(-1, 1, m).astype(np.float32)
+    y = (1.5 / (1 + ((x[None, :] - 0.1) / 0.6) ** 2) + 0.01 * rng.normal(size=(16, m))).astype(np.float32)
+    lo = np.array([0, -1, 1e-3], np.float32)
+    hi = np.array([np.inf, 1, 2], np.float32)
+    got = bf.fit(x, y, "lorentzian", None, (lo, hi), "cuda")
+    ref = oracle.fit("port", "lorentzian", x, y, None, lo, hi, np.float64)
+    np.testing.assert_array_equal(got.status, ref.status)
+    p0 = np.array([1.4, 0.0, 0.5], np.float32)
+    got = bf.fit(x, y, "lorentzian", p0, (lo, hi), "cuda", policy="reference")
+    ref = oracle.fit("port", "lorentzian", x, y, np.tile(p0, (16, 1)), lo, hi, np.float32)
+    np.testing.assert_array_equal(got.status, ref.status)
+    ok = ref.status == 0
+    np.testing.assert_allclose(got.params[ok], ref.params[ok], atol=2e-4, rtol=2e-4)
