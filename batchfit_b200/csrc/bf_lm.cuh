@@ -83,11 +83,14 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
 #pragma unroll
     for (int i = 0; i < TP; ++i)
         aa[i] = 0.0f;
-    // Full chunks without per-point bounds checks, then one masked tail chunk.
+    // Each lane takes kChunk consecutive points per chunk (one 128-bit load of y and
+    // of x when both are 16-byte aligned, as staged rows are); full chunks run
+    // without per-point bounds checks, then one masked tail chunk.
+    static_assert(kChunk == 4, "one float4 per chunk");
     const int full = m - m % (G * kChunk);
-    auto point = [&](int j, float (&part)[KC]) {
+    auto point = [&](float xj, float yj, float (&part)[KC]) {
         float J[P];
-        const float r = Model<MODEL>::residual(q, xs[j], ys[j], J);
+        const float r = Model<MODEL>::residual(q, xj, yj, J);
         part[0] = fmaf(r, r, part[0]);
 #pragma unroll
         for (int k = 0; k < P; ++k) {
@@ -107,15 +110,32 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
             hi[i] = next;
         }
     };
-    for (int base = int(g.lane); base < full; base += G * kChunk) {
-        float part[KC];
+    const bool vec = ((reinterpret_cast<uintptr_t>(xs) | reinterpret_cast<uintptr_t>(ys)) & 15u) == 0u;
+    if (vec) {
+        const float4 *x4 = reinterpret_cast<const float4 *>(xs), *y4 = reinterpret_cast<const float4 *>(ys);
+        for (int base = int(g.lane) * kChunk; base < full; base += G * kChunk) {
+            float part[KC];
 #pragma unroll
-        for (int i = 0; i < KC; ++i)
-            part[i] = 0.0f;
+            for (int i = 0; i < KC; ++i)
+                part[i] = 0.0f;
+            const float4 xv = x4[base / kChunk], yv = y4[base / kChunk];
+            point(xv.x, yv.x, part);
+            point(xv.y, yv.y, part);
+            point(xv.z, yv.z, part);
+            point(xv.w, yv.w, part);
+            fold(part);
+        }
+    } else {
+        for (int base = int(g.lane) * kChunk; base < full; base += G * kChunk) {
+            float part[KC];
 #pragma unroll
-        for (int c = 0; c < kChunk; ++c)
-            point(base + c * G, part);
-        fold(part);
+            for (int i = 0; i < KC; ++i)
+                part[i] = 0.0f;
+#pragma unroll
+            for (int c = 0; c < kChunk; ++c)
+                point(xs[base + c], ys[base + c], part);
+            fold(part);
+        }
     }
     if (full < m) {
         float part[KC];
@@ -124,9 +144,9 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
             part[i] = 0.0f;
 #pragma unroll
         for (int c = 0; c < kChunk; ++c) {
-            const int j = full + int(g.lane) + c * G;
+            const int j = full + int(g.lane) * kChunk + c;
             if (j < m)
-                point(j, part);
+                point(xs[j], ys[j], part);
         }
         fold(part);
     }
