@@ -64,7 +64,9 @@ constexpr int kChunk = 4;
 // a two-sum reduce-scatter across the group with their low parts.  J^T r decides
 // where the iteration stops (its error moves the fixed point), so it gets the
 // compensation; J^T J only shapes the step and takes a plain reduce-scatter.
-template <int MODEL, int G>
+// kAligned: xs and ys are known to be 16-byte aligned (rows staged in shared
+// memory); otherwise alignment is checked at run time (rows read from global memory).
+template <int MODEL, int G, bool kAligned = false>
 __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, const float *ys, int m,
                                         const float *p, double *state) {
     using L = Layout<MODEL>;
@@ -110,7 +112,7 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
             hi[i] = next;
         }
     };
-    const bool vec = ((reinterpret_cast<uintptr_t>(xs) | reinterpret_cast<uintptr_t>(ys)) & 15u) == 0u;
+    const bool vec = kAligned || ((reinterpret_cast<uintptr_t>(xs) | reinterpret_cast<uintptr_t>(ys)) & 15u) == 0u;
     if (vec) {
         const float4 *x4 = reinterpret_cast<const float4 *>(xs), *y4 = reinterpret_cast<const float4 *>(ys);
         for (int base = int(g.lane) * kChunk; base < full; base += G * kChunk) {
@@ -125,7 +127,7 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
             point(xv.w, yv.w, part);
             fold(part);
         }
-    } else {
+    } else if constexpr (!kAligned) {
         for (int base = int(g.lane) * kChunk; base < full; base += G * kChunk) {
             float part[KC];
 #pragma unroll
