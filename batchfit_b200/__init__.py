@@ -162,7 +162,10 @@ def fit(x, y, model="lorentzian", p0=None, bounds=None, device="auto", *, uncert
     if y.ndim != 2 or y.shape[1] != x.size:
         raise ValueError("y must have shape [N,M] matching x[M]")
     x = np.ascontiguousarray(x, dtype=np.float32)
-    y = np.ascontiguousarray(y, dtype=np.float32)
+    # float16 y is the opt-in half-precision storage (half the copy bytes); the
+    # values are fitted exactly as given, converted to float32 on the GPU.
+    y_format = _capi.BF_Y_FLOAT16 if y.dtype == np.float16 else _capi.BF_Y_FLOAT32
+    y = np.ascontiguousarray(y, dtype=np.float16 if y_format == _capi.BF_Y_FLOAT16 else np.float32)
     n, p = y.shape[0], _PARAMETERS[model]
     if p0 is not None:
         p0 = _real_array(p0, "p0")
@@ -183,7 +186,7 @@ def fit(x, y, model="lorentzian", p0=None, bounds=None, device="auto", *, uncert
     us = np.empty(n, np.int32) if uncertainties else None
     ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
     args = _capi.FitArgs(MODELS[model], n, x.size, ptr(x), ptr(y), ptr(p0), _capi.BF_MEMORY_HOST,
-                         int(bool(uncertainties)), int(group_lanes), opts)
+                         int(bool(uncertainties)), int(group_lanes), opts, y_format)
     outs = _capi.FitOutputs(ptr(params), ptr(status), ptr(iterations), ptr(chi2), ptr(cov), ptr(se), ptr(us))
     ctx.fit(args, outs)
     if uncertainties:
@@ -191,14 +194,14 @@ def fit(x, y, model="lorentzian", p0=None, bounds=None, device="auto", *, uncert
     return FitResult(params, status, iterations, chi2)
 
 
-def _device_segment(x, y, model, p0, bounds, uncertainties, policy, group_lanes, options):
+def _device_segment(x, y, model, p0, bounds, uncertainties, policy, group_lanes, options, half_ok=False):
     """Validate torch CUDA inputs and allocate outputs -> (FitArgs, FitOutputs, result, keep-alive)."""
     import torch  # device-memory inputs come from torch (plumbing only)
 
     if not (isinstance(x, torch.Tensor) and isinstance(y, torch.Tensor)):
         raise TypeError("device inputs must be torch CUDA tensors")
-    if x.dtype != torch.float32 or y.dtype != torch.float32:
-        raise TypeError("device inputs must be float32")
+    if x.dtype != torch.float32 or y.dtype not in (torch.float32,) + ((torch.float16,) if half_ok else ()):
+        raise TypeError("device inputs must be float32" + (" (y may be float16)" if half_ok else ""))
     if y.dim() == 1:
         y = y.reshape(1, -1)
     if x.dim() != 1 or x.numel() == 0 or y.dim() != 2 or y.shape[1] != x.numel():
@@ -226,8 +229,9 @@ def _device_segment(x, y, model, p0, bounds, uncertainties, policy, group_lanes,
     se = torch.empty((n, p), dtype=torch.float32, **kw) if uncertainties else None
     us = torch.empty(n, dtype=torch.int32, **kw) if uncertainties else None
     ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())  # noqa: E731
+    y_format = _capi.BF_Y_FLOAT16 if y.dtype == torch.float16 else _capi.BF_Y_FLOAT32
     args = _capi.FitArgs(MODELS[model], n, x.numel(), ptr(x), ptr(y), ptr(p0), _capi.BF_MEMORY_DEVICE,
-                         int(uncertainties), int(group_lanes), opts)
+                         int(uncertainties), int(group_lanes), opts, y_format)
     outs = _capi.FitOutputs(ptr(params), ptr(status), ptr(iterations), ptr(chi2), ptr(cov), ptr(se), ptr(us))
     if uncertainties:
         result = FitResultWithUncertainties(params, status, iterations, chi2, cov, se, us)
@@ -239,7 +243,8 @@ def _device_segment(x, y, model, p0, bounds, uncertainties, policy, group_lanes,
 def _fit_device(x, y, model, p0, bounds, uncertainties, policy, group_lanes, options):
     import torch
 
-    args, outs, result, keep = _device_segment(x, y, model, p0, bounds, uncertainties, policy, group_lanes, options)
+    args, outs, result, keep = _device_segment(x, y, model, p0, bounds, uncertainties, policy, group_lanes, options,
+                                               half_ok=True)
     device = keep[1].device
     torch.cuda.current_stream(device).synchronize()
     context(device.index or 0).fit(args, outs)

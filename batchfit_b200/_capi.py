@@ -35,6 +35,7 @@ EXPORTS = (
     "bf_server_get_stats", "bf_cuda_fit_npy", "bf_npy_inspect", "bf_cuda_fit_physical",
 )
 
+BF_Y_FLOAT32, BF_Y_FLOAT16 = 0, 1
 BF_BATCH_FIXED_MAPPING = 1
 BF_BATCH_NO_GRAPH = 2
 
@@ -68,6 +69,7 @@ class FitArgs(C.Structure):
         ("uncertainties", C.c_int32),
         ("group_lanes", C.c_int32),
         ("options", SolverOptions),
+        ("y_format", C.c_int32),
     ]
 
 

@@ -19,6 +19,7 @@ struct FitArgs {
     long long n;
     int m;
     int uncertainties;
+    int y_half; // y holds IEEE binary16 values (staged to float32)
     uint32_t max_iterations;
     uint32_t flags;    // kFlagScaledCholesky honoured; sums are always compensated
     uint32_t policy;   // kPolicyReference or kPolicyParity

@@ -103,6 +103,7 @@ bf::FitArgs make_args(const bf_fit_args &in, int p) {
     const bf_solver_options &o = in.options;
     a.m = int(in.m);
     a.uncertainties = in.uncertainties ? 1 : 0;
+    a.y_half = in.y_format == BF_Y_FLOAT16 ? 1 : 0;
     a.max_iterations = o.max_iterations;
     a.flags = (o.compensated_sum ? bf::kFlagCompensated : 0u) | (o.scaled_cholesky ? bf::kFlagScaledCholesky : 0u);
     a.policy = o.policy == BF_POLICY_PARITY ? bf::kPolicyParity : bf::kPolicyReference;
@@ -148,6 +149,8 @@ int validate(const bf_fit_args *args, const bf_fit_outputs *out, uint32_t limit 
         return fail(BF_ERR_INVALID_ARGUMENT, "N*M or N*P*P overflows 64-bit indexing");
     if (args->group_lanes != 0 && args->group_lanes != 8 && args->group_lanes != 16 && args->group_lanes != 32)
         return fail(BF_ERR_INVALID_ARGUMENT, "group_lanes must be 0, 8, 16 or 32");
+    if (args->y_format != BF_Y_FLOAT32 && args->y_format != BF_Y_FLOAT16)
+        return fail(BF_ERR_INVALID_ARGUMENT, "y_format must be BF_Y_FLOAT32 or BF_Y_FLOAT16");
     if (args->n == 0)
         return BF_OK;
     if (!args->x || !args->y)
@@ -179,7 +182,8 @@ int launch_batch(bf_cuda_context *ctx, const bf_fit_args &in, const bf::FitArgs 
     KernelEvents ev{take_event(ctx), take_event(ctx), take_event(ctx), take_event(ctx)};
     BF_CUDA(cudaEventRecord(ev.start, st));
     if (!p0 || guess_only) {
-        BF_CUDA(bf::launch_guess(in.model, x, y, count, int(in.m), guess_buf, guess_status, ctx->sms, st));
+        BF_CUDA(bf::launch_guess(in.model, x, y, count, int(in.m), guess_buf, guess_status, ctx->sms, st,
+                                 base.y_half));
         ++ctx->launches;
         p0 = guess_buf;
     }
@@ -260,13 +264,14 @@ int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &o
     BF_CUDA(cudaStreamWaitEvent(ctx->stream[1], x_ready, 0));
     ctx->event_pool.push_back(x_ready);
     // ~128 MB of observations per chunk, at least a few waves of fits.
-    uint64_t chunk = std::max<uint64_t>(16384, (128ull << 20) / (m * sizeof(float)));
+    const size_t ybytes = in.y_format == BF_Y_FLOAT16 ? 2 : sizeof(float); // bytes per y value
+    uint64_t chunk = std::max<uint64_t>(16384, (128ull << 20) / (m * ybytes));
     if (chunk > n)
         chunk = n;
     const bool has_p0 = in.p0 != nullptr;
     for (int i = 0; i < kSlots && n > 0; ++i) {
         Slot &s = ctx->slot[i];
-        BF_CUDA(s.y.reserve(chunk * m * sizeof(float)));
+        BF_CUDA(s.y.reserve(chunk * m * ybytes));
         if (has_p0)
             BF_CUDA(s.p0.reserve(chunk * p * sizeof(float)));
         else
@@ -287,7 +292,8 @@ int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &o
         const uint64_t count = std::min(chunk, n - first);
         Slot &s = ctx->slot[c % kSlots];
         cudaStream_t st = ctx->stream[c % kSlots];
-        BF_CUDA(cudaMemcpyAsync(s.y.ptr, in.y + first * m, count * m * sizeof(float), cudaMemcpyHostToDevice, st));
+        BF_CUDA(cudaMemcpyAsync(s.y.ptr, reinterpret_cast<const char *>(in.y) + first * m * ybytes,
+                                count * m * ybytes, cudaMemcpyHostToDevice, st));
         if (has_p0)
             BF_CUDA(cudaMemcpyAsync(s.p0.ptr, in.p0 + first * p, count * p * sizeof(float), cudaMemcpyHostToDevice,
                                     st));
@@ -367,6 +373,8 @@ int prepare_segment(const bf_fit_args *args, const bf_fit_outputs *out, uint32_t
     const int rc = validate(args, out, max_points);
     if (rc != BF_OK)
         return rc;
+    if (args->y_format != BF_Y_FLOAT32)
+        return fail(BF_ERR_INVALID_ARGUMENT, "this entry point takes float32 y (BF_Y_FLOAT32)");
     *base = make_args(*args, parameter_count(args->model));
     return BF_OK;
 }

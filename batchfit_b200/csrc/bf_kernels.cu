@@ -110,7 +110,8 @@ __device__ void cta_prologue(const float *x, int m, float *xs, XConst &xc) {
 // shared-memory sorting path for very long spectra).
 template <int MODEL, int G, int V>
 __global__ void __launch_bounds__(GuessShapeCfg<V>::threads, GuessShapeCfg<V>::min_blocks) guess_kernel(const float *x, const float *y, long long n,
-                                                                   int m, float *guesses, int32_t *guess_status) {
+                                                                   int m, float *guesses, int32_t *guess_status,
+                                                                   int y_half) {
     constexpr int P = Model<MODEL>::P;
     constexpr int kGroups = GuessShapeCfg<V>::threads / G;
     extern __shared__ __align__(16) float smem[];
@@ -122,11 +123,11 @@ __global__ void __launch_bounds__(GuessShapeCfg<V>::threads, GuessShapeCfg<V>::m
     const int gid = threadIdx.x / G;
     float *ys = smem + x_words(m) + gid * guess_group_words(m, G, V);
     float *scratch = ys + round_up(m, 4);
-    const bool vec_ok = (m & 3) == 0 && (reinterpret_cast<uintptr_t>(y) & 15) == 0;
+    const bool vec_ok = rows_vectorisable(y, m, y_half);
     for (long long fit = (long long)blockIdx.x * kGroups + gid; fit < n; fit += (long long)gridDim.x * kGroups) {
         bool yfin, flat;
         float syy;
-        stage_row(g, y + fit * (long long)m, m, vec_ok, ys, yfin, flat, syy);
+        stage_fit_row(g, y, y_half, fit, m, vec_ok, ys, yfin, flat, syy);
         float p[P];
         const int gs = initial_guess<MODEL, G, V>(g, cx, xs, ys, yfin, scratch, p);
 #pragma unroll
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(LmShape<MODEL>::threads, LmShape<MODEL>::min_b
     const int gid = threadIdx.x / G;
     float *ys = smem + x_words(m) + gid * lm_group_words<MODEL>(m, G);
     double *state = reinterpret_cast<double *>(ys + round_up(m, 4));
-    const bool vec_ok = (m & 3) == 0 && (reinterpret_cast<uintptr_t>(a.y) & 15) == 0;
+    const bool vec_ok = rows_vectorisable(a.y, m, a.y_half);
     long long next_static = (long long)blockIdx.x * kGroups + gid;
     LmState<MODEL> s;
     long long fit = -1;
@@ -177,7 +178,7 @@ __global__ void __launch_bounds__(LmShape<MODEL>::threads, LmShape<MODEL>::min_b
                 if (f >= a.n)
                     break;
                 bool yfin;
-                stage_row(g, a.y + f * (long long)m, m, vec_ok, ys, yfin, flat, syy);
+                stage_fit_row(g, a.y, a.y_half, f, m, vec_ok, ys, yfin, flat, syy);
                 bool init_finite = true;
 #pragma unroll
                 for (int k = 0; k < P; ++k) {
@@ -380,14 +381,14 @@ static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t strea
 
 template <int MODEL, int G, int V>
 static cudaError_t launch_guess_typed(const float *x, const float *y, long long n, int m, float *guesses,
-                                      int32_t *status, int sms, cudaStream_t stream) {
+                                      int32_t *status, int sms, cudaStream_t stream, int y_half) {
     const int smem = guess_smem_bytes<G, V>(m);
     int grid = 0, per_sm = 0;
     constexpr int kThreads = GuessShapeCfg<V>::threads;
     cudaError_t e = grid_for(guess_kernel<MODEL, G, V>, kThreads, smem, n, kThreads / G, sms, grid, per_sm);
     if (e != cudaSuccess)
         return e;
-    guess_kernel<MODEL, G, V><<<grid, kThreads, smem, stream>>>(x, y, n, m, guesses, status);
+    guess_kernel<MODEL, G, V><<<grid, kThreads, smem, stream>>>(x, y, n, m, guesses, status, y_half);
     return cudaGetLastError();
 }
 
@@ -419,17 +420,17 @@ static cudaError_t launch_lm_model(const FitArgs &a, int lanes, int sms, cudaStr
 
 template <int MODEL>
 static cudaError_t launch_guess_model(const float *x, const float *y, long long n, int m, float *guesses,
-                                      int32_t *status, int sms, cudaStream_t s) {
+                                      int32_t *status, int sms, cudaStream_t s, int y_half) {
     const GuessShape gs = guess_shape(m);
     switch (gs.lanes * 100 + gs.v) {
-    case 801: return launch_guess_typed<MODEL, 8, 1>(x, y, n, m, guesses, status, sms, s);
-    case 802: return launch_guess_typed<MODEL, 8, 2>(x, y, n, m, guesses, status, sms, s);
-    case 804: return launch_guess_typed<MODEL, 8, 4>(x, y, n, m, guesses, status, sms, s);
-    case 808: return launch_guess_typed<MODEL, 8, 8>(x, y, n, m, guesses, status, sms, s);
-    case 816: return launch_guess_typed<MODEL, 8, 16>(x, y, n, m, guesses, status, sms, s);
-    case 1616: return launch_guess_typed<MODEL, 16, 16>(x, y, n, m, guesses, status, sms, s);
-    case 3216: return launch_guess_typed<MODEL, 32, 16>(x, y, n, m, guesses, status, sms, s);
-    default: return launch_guess_typed<MODEL, 32, 0>(x, y, n, m, guesses, status, sms, s);
+    case 801: return launch_guess_typed<MODEL, 8, 1>(x, y, n, m, guesses, status, sms, s, y_half);
+    case 802: return launch_guess_typed<MODEL, 8, 2>(x, y, n, m, guesses, status, sms, s, y_half);
+    case 804: return launch_guess_typed<MODEL, 8, 4>(x, y, n, m, guesses, status, sms, s, y_half);
+    case 808: return launch_guess_typed<MODEL, 8, 8>(x, y, n, m, guesses, status, sms, s, y_half);
+    case 816: return launch_guess_typed<MODEL, 8, 16>(x, y, n, m, guesses, status, sms, s, y_half);
+    case 1616: return launch_guess_typed<MODEL, 16, 16>(x, y, n, m, guesses, status, sms, s, y_half);
+    case 3216: return launch_guess_typed<MODEL, 32, 16>(x, y, n, m, guesses, status, sms, s, y_half);
+    default: return launch_guess_typed<MODEL, 32, 0>(x, y, n, m, guesses, status, sms, s, y_half);
     }
 }
 
@@ -445,12 +446,12 @@ cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStre
 }
 
 cudaError_t launch_guess(int model, const float *x, const float *y, long long n, int m, float *guesses,
-                         int32_t *status, int sms, cudaStream_t s) {
+                         int32_t *status, int sms, cudaStream_t s, int y_half) {
     switch (model) {
-    case kGaussian: return launch_guess_model<kGaussian>(x, y, n, m, guesses, status, sms, s);
-    case kLorentzian: return launch_guess_model<kLorentzian>(x, y, n, m, guesses, status, sms, s);
-    case kPseudoVoigt: return launch_guess_model<kPseudoVoigt>(x, y, n, m, guesses, status, sms, s);
-    case kTwoLorentzian: return launch_guess_model<kTwoLorentzian>(x, y, n, m, guesses, status, sms, s);
+    case kGaussian: return launch_guess_model<kGaussian>(x, y, n, m, guesses, status, sms, s, y_half);
+    case kLorentzian: return launch_guess_model<kLorentzian>(x, y, n, m, guesses, status, sms, s, y_half);
+    case kPseudoVoigt: return launch_guess_model<kPseudoVoigt>(x, y, n, m, guesses, status, sms, s, y_half);
+    case kTwoLorentzian: return launch_guess_model<kTwoLorentzian>(x, y, n, m, guesses, status, sms, s, y_half);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -14,9 +14,9 @@ cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStre
                        cudaEvent_t lm_done = nullptr);
 
 // Launch the data-only guess kernel: guesses[N*P] and, when non-null, status[N].
-// Its group width follows from M.
+// Its group width follows from M; y_half: y holds IEEE binary16 values.
 cudaError_t launch_guess(int model, const float *x, const float *y, long long n, int m, float *guesses,
-                         int32_t *status, int sms, cudaStream_t stream);
+                         int32_t *status, int sms, cudaStream_t stream, int y_half = 0);
 
 // Dynamic shared memory of one CTA for (model, lanes, M).
 int smem_bytes(int model, int lanes, int m);

@@ -18,6 +18,7 @@
 #pragma once
 
 #include "bf_args.h"
+#include <cuda_fp16.h>
 #include "bf_device.cuh"
 #include "bf_guess.cuh"
 #include "bf_models.cuh"
@@ -640,6 +641,60 @@ __device__ __forceinline__ void stage_row(const Group<G> &g, const float *row, i
     for (int o = G / 2; o >= 1; o >>= 1)
         syy += g.xor_(syy, o);
     g.sync();
+}
+
+// A row of y stored as IEEE binary16 (opt-in half-precision storage), converted
+// exactly to float32 while it is staged, with stage_row's accumulations in the same
+// order: a fit of half-precision y equals the fit of the same values given as float.
+template <int G>
+__device__ __forceinline__ void stage_row_half(const Group<G> &g, const __half *row, int m, bool vec_ok, float *ys,
+                                               bool &yfin, bool &flat, float &syy) {
+    const float y0 = __half2float(row[0]);
+    yfin = true;
+    flat = true;
+    syy = 0.0f;
+    if (vec_ok) {
+        const uint2 *row4 = reinterpret_cast<const uint2 *>(row);
+        for (int v = int(g.lane); v < m / 4; v += G) {
+            const uint2 raw = __ldcs(row4 + v);
+            const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&raw.x));
+            const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&raw.y));
+            const float4 t = make_float4(a.x, a.y, b.x, b.y);
+            reinterpret_cast<float4 *>(ys)[v] = t;
+            yfin = yfin && isfinite(t.x) && isfinite(t.y) && isfinite(t.z) && isfinite(t.w);
+            flat = flat && t.x == y0 && t.y == y0 && t.z == y0 && t.w == y0;
+            syy = fmaf(t.x, t.x, fmaf(t.y, t.y, fmaf(t.z, t.z, fmaf(t.w, t.w, syy))));
+        }
+    } else {
+        for (int j = int(g.lane); j < m; j += G) {
+            const float t = __half2float(row[j]);
+            ys[j] = t;
+            yfin = yfin && isfinite(t);
+            flat = flat && t == y0;
+            syy = fmaf(t, t, syy);
+        }
+    }
+    yfin = g.all(yfin);
+    flat = g.all(flat);
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1)
+        syy += g.xor_(syy, o);
+    g.sync();
+}
+
+// Whether rows of y start 128-bit (float) / 64-bit (half) aligned: 4 values a load.
+__device__ __forceinline__ bool rows_vectorisable(const float *y, int m, bool y_half) {
+    return (m & 3) == 0 && (reinterpret_cast<uintptr_t>(y) & (y_half ? 7u : 15u)) == 0;
+}
+
+// Stage row `fit` of y (float32, or binary16 when y_half) into shared memory.
+template <int G>
+__device__ __forceinline__ void stage_fit_row(const Group<G> &g, const float *y, bool y_half, long long fit, int m,
+                                              bool vec_ok, float *ys, bool &yfin, bool &flat, float &syy) {
+    if (y_half)
+        stage_row_half<G>(g, reinterpret_cast<const __half *>(y) + fit * m, m, vec_ok, ys, yfin, flat, syy);
+    else
+        stage_row<G>(g, y + fit * m, m, vec_ok, ys, yfin, flat, syy);
 }
 
 // Covariance of one finished fit from the information matrix the LM kernel left in

@@ -79,6 +79,8 @@ int bf_cuda_fit_noalloc(const bf_fit_args *args, const bf_fit_outputs *out, void
         return rc;
     if (args->memory != BF_MEMORY_DEVICE)
         return bf::host::report(BF_ERR_INVALID_ARGUMENT, "bf_cuda_fit_noalloc takes device memory only");
+    if (args->y_format != BF_Y_FLOAT32)
+        return bf::host::report(BF_ERR_INVALID_ARGUMENT, "bf_cuda_fit_noalloc takes float32 y");
     if (!args->p0 && args->n > max_guessed_fits(args->model))
         return bf::host::report(
             BF_ERR_INVALID_ARGUMENT,

@@ -53,6 +53,15 @@ extern "C" {
 #define BF_MEMORY_HOST 0   /* host memory (pinned memory overlaps copies with compute) */
 #define BF_MEMORY_DEVICE 1 /* device memory of the context's GPU */
 
+/* Storage of y.  BF_Y_FLOAT16 is an opt-in half-precision storage, like the
+ * reference's profiling variant (src/metal/profile_variants.metal:12-15): y holds
+ * IEEE binary16 values, which halves y's host-to-device and HBM bytes; each value
+ * is converted exactly to float32 on the GPU, so the fit equals the float32 fit of
+ * the same (already rounded) values.  Accepted by bf_cuda_fit and bf_cuda_submit;
+ * the other entry points take float32 y. */
+#define BF_Y_FLOAT32 0
+#define BF_Y_FLOAT16 1
+
 /* Stopping policy.
  * BF_POLICY_REFERENCE: the reference float solver's stop rules with the given
  *   tolerances (defaults 1e-5 / 1e-6 / 1e-6).
@@ -89,6 +98,7 @@ typedef struct bf_fit_args {
     int32_t uncertainties;
     int32_t group_lanes; /* 0 = tuned choice, else 8, 16 or 32 lanes per fit */
     bf_solver_options options;
+    int32_t y_format;    /* BF_Y_FLOAT32, or BF_Y_FLOAT16 (bf_cuda_fit / submit only) */
 } bf_fit_args;
 
 typedef struct bf_fit_outputs {

@@ -371,3 +371,22 @@ def test_tiny_spectra_match_the_oracle(bf, oracle, m):
     np.testing.assert_array_equal(got.status, ref.status)
     ok = ref.status == 0
     np.testing.assert_allclose(got.params[ok], ref.params[ok], atol=2e-4, rtol=2e-4)
+
+
+def test_half_precision_y_equals_float_of_the_same_values(bf):
+    """Opt-in half-precision storage of y (BF_Y_FLOAT16): the fit of binary16 y
+    equals, bit for bit, the fit of the same values converted to float32, host and
+    device memory, aligned (M % 4 == 0) and ragged rows; other entry points refuse it."""
+    import torch
+
+    for m in (256, 131):
+        x, y, lo, hi = synthetic("pseudo_voigt", 300, m, seed=m)
+        y16 = y.astype(np.float16)
+        half = bf.fit(x, y16, "pseudo_voigt", None, (lo, hi), "cuda", uncertainties=True)
+        full = bf.fit(x, y16.astype(np.float32), "pseudo_voigt", None, (lo, hi), "cuda", uncertainties=True)
+        for k in half._fields:
+            np.testing.assert_array_equal(getattr(half, k), getattr(full, k), err_msg=f"M={m} {k}")
+        dev = bf.fit(torch.as_tensor(x).cuda(), torch.as_tensor(y16).cuda(), "pseudo_voigt", None, (lo, hi), "cuda")
+        np.testing.assert_array_equal(dev.params.cpu().numpy(), full.params)
+    with pytest.raises(TypeError):
+        bf.fit_batch([dict(x=torch.as_tensor(x).cuda(), y=torch.as_tensor(y16).cuda(), model="pseudo_voigt")])
