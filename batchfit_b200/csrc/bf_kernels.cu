@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(LmShape<MODEL>::threads, LmShape<MODEL>::min_b
             if (fit < 0)
                 break;
         }
-        const bool pass_finite = lm_pass<MODEL, G, true>(g, xs, ys, m, s.t, state + (1 - s.cur) * Layout<MODEL>::K);
+        const bool pass_finite = lm_pass<MODEL, G>(g, xs, ys, m, s.t, state + (1 - s.cur) * Layout<MODEL>::K);
         bool done = lm_after_pass<MODEL, G>(g, a, cx, flat, pass_finite, state, s);
         if (!done)
             done = lm_plan<MODEL>(a, cx, double(syy), state, s);

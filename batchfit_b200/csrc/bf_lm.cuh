@@ -65,9 +65,7 @@ constexpr int kChunk = 4;
 // a two-sum reduce-scatter across the group with their low parts.  J^T r decides
 // where the iteration stops (its error moves the fixed point), so it gets the
 // compensation; J^T J only shapes the step and takes a plain reduce-scatter.
-// kAligned: xs and ys are known to be 16-byte aligned (rows staged in shared
-// memory); otherwise alignment is checked at run time (rows read from global memory).
-template <int MODEL, int G, bool kAligned = false>
+template <int MODEL, int G>
 __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, const float *ys, int m,
                                         const float *p, double *state) {
     using L = Layout<MODEL>;
@@ -86,14 +84,11 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
 #pragma unroll
     for (int i = 0; i < TP; ++i)
         aa[i] = 0.0f;
-    // Each lane takes kChunk consecutive points per chunk (one 128-bit load of y and
-    // of x when both are 16-byte aligned, as staged rows are); full chunks run
-    // without per-point bounds checks, then one masked tail chunk.
-    static_assert(kChunk == 4, "one float4 per chunk");
+    // Full chunks without per-point bounds checks, then one masked tail chunk.
     const int full = m - m % (G * kChunk);
-    auto point = [&](float xj, float yj, float (&part)[KC]) {
+    auto point = [&](int j, float (&part)[KC]) {
         float J[P];
-        const float r = Model<MODEL>::residual(q, xj, yj, J);
+        const float r = Model<MODEL>::residual(q, xs[j], ys[j], J);
         part[0] = fmaf(r, r, part[0]);
 #pragma unroll
         for (int k = 0; k < P; ++k) {
@@ -113,32 +108,15 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
             hi[i] = next;
         }
     };
-    const bool vec = kAligned || ((reinterpret_cast<uintptr_t>(xs) | reinterpret_cast<uintptr_t>(ys)) & 15u) == 0u;
-    if (vec) {
-        const float4 *x4 = reinterpret_cast<const float4 *>(xs), *y4 = reinterpret_cast<const float4 *>(ys);
-        for (int base = int(g.lane) * kChunk; base < full; base += G * kChunk) {
-            float part[KC];
+    for (int base = int(g.lane); base < full; base += G * kChunk) {
+        float part[KC];
 #pragma unroll
-            for (int i = 0; i < KC; ++i)
-                part[i] = 0.0f;
-            const float4 xv = x4[base / kChunk], yv = y4[base / kChunk];
-            point(xv.x, yv.x, part);
-            point(xv.y, yv.y, part);
-            point(xv.z, yv.z, part);
-            point(xv.w, yv.w, part);
-            fold(part);
-        }
-    } else if constexpr (!kAligned) {
-        for (int base = int(g.lane) * kChunk; base < full; base += G * kChunk) {
-            float part[KC];
+        for (int i = 0; i < KC; ++i)
+            part[i] = 0.0f;
 #pragma unroll
-            for (int i = 0; i < KC; ++i)
-                part[i] = 0.0f;
-#pragma unroll
-            for (int c = 0; c < kChunk; ++c)
-                point(xs[base + c], ys[base + c], part);
-            fold(part);
-        }
+        for (int c = 0; c < kChunk; ++c)
+            point(base + c * G, part);
+        fold(part);
     }
     if (full < m) {
         float part[KC];
@@ -147,9 +125,9 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
             part[i] = 0.0f;
 #pragma unroll
         for (int c = 0; c < kChunk; ++c) {
-            const int j = full + int(g.lane) * kChunk + c;
+            const int j = full + int(g.lane) + c * G;
             if (j < m)
-                point(xs[j], ys[j], part);
+                point(j, part);
         }
         fold(part);
     }

@@ -221,11 +221,16 @@ struct Writer {
     }
 };
 
-// Read `count` values starting at element `first` of an NPY payload as float32.
+// Read `count` values starting at element `first` of an NPY payload as float32
+// (float64 payloads go through `tmp` and are rounded to nearest).
 bool read_floats(int fd, const Header &h, uint64_t first, uint64_t count, float *out, std::vector<double> &tmp) {
+    char *dst = reinterpret_cast<char *>(out);
+    if (h.dtype == 1) {
+        tmp.resize(count);
+        dst = reinterpret_cast<char *>(tmp.data());
+    }
     const off_t off = off_t(h.offset + first * h.item);
     const size_t bytes = size_t(count * h.item);
-    char *dst = h.dtype == 1 ? reinterpret_cast<char *>((tmp.resize(count), tmp.data())) : reinterpret_cast<char *>(out);
     size_t done = 0;
     while (done < bytes) {
         const ssize_t r = pread(fd, dst + done, bytes - done, off + off_t(done));
