@@ -303,7 +303,8 @@ bool batch_guess_shape(int m, int *lanes, int *v) {
         *lanes = 32;
         *v = 0;
     }
-    return n1 <= kBatchMaxSortWidth;
+    // The per-group share of the warp buffer holds the sort and the second-peak arrays.
+    return n1 <= kBatchMaxSortWidth && second_peak_words(m, *lanes) <= kGuessWarpFloats / (32 / *lanes);
 }
 
 cudaError_t launch_synthetic(int model, int m, long long n, unsigned seed, float *x, float *y,

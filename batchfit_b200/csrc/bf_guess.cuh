@@ -129,12 +129,20 @@ __device__ __forceinline__ float sorted_median(const float *a, int n) {
     return (n & 1) ? a[n / 2] : midpoint_rn(a[n / 2 - 1], a[n / 2]);
 }
 
-template <int MODEL> struct Signal {
-    // signal[j] = y[j] - (level + slope*(x[j]-left_x))   (initial_guess.hpp:158-162)
+// signal[j] = y[j] - (level + slope*(x[j]-left_x))   (initial_guess.hpp:158-162).
+// PRE: ys already holds the signal (the guess kernel overwrites its staged copy of
+// the row once, with exactly these roundings), so a sample is one load.
+template <int MODEL, bool PRE = false> struct Signal {
     const float *xs, *ys;
     float level, slope, left_x;
     int m;
     __device__ __forceinline__ float at(int j) const {
+        if constexpr (PRE)
+            return ys[j];
+        else
+            return raw_at(j);
+    }
+    __device__ __forceinline__ float raw_at(int j) const {
         if constexpr (Model<MODEL>::paired)
             return rsub(ys[j], radd(level, rmul(slope, rsub(xs[j], left_x))));
         else
@@ -170,8 +178,8 @@ template <int MODEL> struct Signal {
 // neighbour is carried from the previous chunk; the last lane computes its right
 // neighbour).  Two chunks are in flight per step.  f(j, value, left, right) runs on
 // lanes with an interior j.  Returns whether every signal sample is finite.
-template <int MODEL, int G, class F>
-__device__ __forceinline__ bool scan_smoothed(const Group<G> &g, const Signal<MODEL> &s, F &&f) {
+template <int G, class S, class F>
+__device__ __forceinline__ bool scan_smoothed(const Group<G> &g, const S &s, F &&f) {
     const int m = s.m;
     const float first = s.at(0);
     float carry = first; // smooth(0) is the raw edge sample
@@ -227,8 +235,8 @@ struct PeakFeature {
 
 // detail::peak (initial_guess.hpp:61-109) with the half-height walks done as
 // group-parallel searches for the nearest sample at or below half height.
-template <int MODEL, int G>
-__device__ PeakFeature find_peak(const Group<G> &g, const Signal<MODEL> &s, const float *xs, int index,
+template <int G, class S>
+__device__ PeakFeature find_peak(const Group<G> &g, const S &s, const float *xs, int index,
                                  int begin, int end, bool mirror) {
     PeakFeature r{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, false};
     r.amplitude = s.at(index);
@@ -304,8 +312,18 @@ __device__ PeakFeature find_peak(const Group<G> &g, const Signal<MODEL> &s, cons
 // (bmin, bmax, pmin, smin: four arrays of ceil(M/32) floats, back to back).  Lane l
 // takes blocks l, l+G, ...
 constexpr int kWalkBlock = 32;
-template <int MODEL, int G>
-__device__ void block_extrema(const Group<G> &g, const Signal<MODEL> &s, float *bmin, float *bmax) {
+__host__ __device__ inline int walk_blocks(int m) { return (m + kWalkBlock - 1) / kWalkBlock; }
+// Interior samples j = 1 + lane + k*G (j <= m - 2) of one group lane.
+__host__ __device__ inline int lane_samples(int m, int lane, int lanes) {
+    return m - 3 - lane >= 0 ? (m - 3 - lane) / lanes + 1 : 0;
+}
+// Scratch words of the second-peak search: four block arrays, then one candidate
+// bit per interior sample (lane-wise words, word-major).
+__host__ __device__ inline int second_peak_words(int m, int lanes) {
+    return 4 * walk_blocks(m) + lanes * ((lane_samples(m, 0, lanes) + 31) / 32);
+}
+template <int G, class S>
+__device__ void block_extrema(const Group<G> &g, const S &s, float *bmin, float *bmax) {
     const int blocks = (s.m + kWalkBlock - 1) / kWalkBlock;
     for (int b = int(g.lane); b < blocks; b += G) {
         const int first = b * kWalkBlock, end = min(s.m, first + kWalkBlock);
@@ -354,8 +372,8 @@ __device__ __forceinline__ bool may_be_prominent(const float *pmin, const float 
 // sides some sample of the walk has height - sample > threshold.  Each walk stops
 // at its first such sample (side passes) or at the reference's stop (side fails),
 // and crosses whole blocks whose maximum is at most the height by their minimum.
-template <int MODEL>
-__device__ bool prominent(const Signal<MODEL> &s, const float *bmin, const float *bmax, int index,
+template <class S>
+__device__ bool prominent(const S &s, const float *bmin, const float *bmax, int index,
                           float threshold) {
     const float height = s.smooth(index);
     bool left = false;
@@ -402,7 +420,7 @@ __device__ bool prominent(const Signal<MODEL> &s, const float *bmin, const float
 // V > 0: edge medians sorted in registers, G*V >= max(1, M/10) values per side;
 // V == 0: the general shared-memory path (any M).  `scratch` holds
 // 2*max(n1, G*V) floats.
-template <int MODEL, int G, int V>
+template <int MODEL, int G, int V, bool PRE = false>
 __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *xs, const float *ys,
                              bool y_finite, float *scratch, float *out) {
     constexpr int P = Model<MODEL>::P;
@@ -500,20 +518,50 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
     }
     if (!isfinite(slope))
         return kGuessInvalid;
-    const Signal<MODEL> s{xs, ys, level, slope, xc.left_x, m};
     // Noise scale: 1.4826 * median of absolute edge deviations (initial_guess.hpp:163-169).
     const float noise = rmul(1.4826f, noise_median);
     if (!isfinite(noise))
         return kGuessInvalid;
+    if constexpr (PRE) {
+        // ys is this group's own staged, 16-byte aligned copy of the row (padded to
+        // a multiple of 4 floats, as is xs): overwrite it with the signal.
+        const Signal<MODEL> raw{xs, ys, level, slope, xc.left_x, m};
+        float4 *row = reinterpret_cast<float4 *>(const_cast<float *>(ys));
+        for (int q = int(g.lane); 4 * q < m; q += G) {
+            float4 v;
+            v.x = raw.raw_at(4 * q);
+            v.y = raw.raw_at(4 * q + 1);
+            v.z = raw.raw_at(4 * q + 2);
+            v.w = raw.raw_at(4 * q + 3);
+            row[q] = v;
+        }
+        g.sync();
+    }
+    const Signal<MODEL, PRE> s{xs, ys, level, slope, xc.left_x, m};
     // Tallest smoothed local maximum (initial_guess.hpp:170-179).  The same sweep
     // checks that every signal sample is finite (initial_guess.hpp:158-162); both
-    // failures end in invalid_input, so their order does not matter.
+    // failures end in invalid_input, so their order does not matter.  For the
+    // two-Lorentzian it also records every positive smoothed local maximum, the
+    // candidates of the second-peak search, as one bit per sample of the lane
+    // (lane l visits j = 1 + l + k*G: bit k of word k/32, words stored
+    // word-major after the block extrema in `scratch`).
     float height = 0.0f;
     int first = m;
-    const bool signal_finite = scan_smoothed<MODEL, G>(g, s, [&](int j, float v, float left, float right) {
-        if (v > 0.0f && v > left && v >= right && v > height) {
+    [[maybe_unused]] unsigned *cand_bits = reinterpret_cast<unsigned *>(scratch + 4 * walk_blocks(m));
+    [[maybe_unused]] unsigned word = 0;
+    const bool signal_finite = scan_smoothed<G>(g, s, [&](int j, float v, float left, float right) {
+        const bool peak = v > 0.0f && v > left && v >= right;
+        if (peak && v > height) {
             height = v;
             first = j;
+        }
+        if constexpr (paired) {
+            const int k = int(unsigned(j - 1 - int(g.lane)) / G);
+            word |= unsigned(peak) << (k & 31);
+            if ((k & 31) == 31 || j + G + 1 >= m) {
+                cand_bits[(k >> 5) * G + int(g.lane)] = word;
+                word = 0;
+            }
         }
     });
     if (!g.all(signal_finite))
@@ -522,7 +570,7 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
     if (first == m || height <= rmul(3.0f, noise))
         return kGuessNoPeak;
     first = s.raw_maximum(first);
-    PeakFeature primary = find_peak<MODEL, G>(g, s, xs, first, 0, m - 1, false);
+    PeakFeature primary = find_peak<G>(g, s, xs, first, 0, m - 1, false);
     if (!primary.valid)
         return kGuessNoPeak;
     if constexpr (!paired) {
@@ -539,44 +587,51 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
     } else {
         // Second peak (initial_guess.hpp:199-227): the tallest smoothed local maximum
         // (ties: smaller index) that is far enough from the first and prominent
-        // enough.  One sweep collects each lane's two best candidates.  The best of
-        // the lanes' second candidates is a cut-off: every candidate better than it
-        // is some lane's first, so the candidates at or above the cut-off are the
-        // true leaders.  Each lane tests its own leaders; the best passing one is the
-        // answer.  When all fail, a second sweep tests every candidate below the
-        // cut-off, each lane its own indices, and keeps the best passing one.
+        // enough.  The candidates are the positive smoothed local maxima the first
+        // sweep recorded (bits per lane).  One walk over each lane's candidates
+        // collects its two best far-enough ones.  The best of the lanes' second
+        // candidates is a cut-off: every candidate better than it is some lane's
+        // first, so the candidates at or above the cut-off are the true leaders.
+        // Each lane tests its own leaders; the best passing one is the answer.  When
+        // all fail, the lanes test every candidate below the cut-off and keep the
+        // best passing one.
         const float separation =
             smax(rmul(3.0f, xc.guess_spacing), rmul(2.0f, smin(primary.left_radius, primary.right_radius)));
         const float threshold = rmul(3.0f, noise);
-        // The edge runs are no longer needed: their buffer holds the block extrema.
-        const int blocks = (m + kWalkBlock - 1) / kWalkBlock;
+        // The edge runs are no longer needed: their buffer holds the block extrema
+        // (the candidate bits follow them).
+        const int blocks = walk_blocks(m);
         float *bmin = scratch, *bmax = bmin + blocks, *pmin = bmax + blocks, *smin = pmin + blocks;
-        block_extrema<MODEL, G>(g, s, bmin, bmax);
+        block_extrema<G>(g, s, bmin, bmax);
         auto far_enough = [&](int j) {
             const int idx = s.raw_maximum(j);
             const int bins = idx > first ? idx - first : first - idx;
             return !(bins < 3 || fabsf(rsub(xs[idx], primary.center)) < separation);
         };
+        const int words = (lane_samples(m, int(g.lane), G) + 31) >> 5;
+        const unsigned *bits = cand_bits + int(g.lane);
         int second = m;
         float v1 = 0.0f, v2 = 0.0f;
         int j1 = m, j2 = m;
-        scan_smoothed<MODEL, G>(g, s, [&](int j, float v, float left, float right) {
-            if (!(v > 0.0f && v > left && v >= right))
-                return;
-            if (!(v > v2 || (v == v2 && j < j2)))
-                return;
-            if (!far_enough(j))
-                return;
-            if (v > v1 || (v == v1 && j < j1)) {
-                v2 = v1;
-                j2 = j1;
-                v1 = v;
-                j1 = j;
-            } else {
-                v2 = v;
-                j2 = j;
+        for (int w = 0; w < words; ++w) {
+            unsigned cand = bits[w * G];
+            while (cand) {
+                const int j = 1 + int(g.lane) + (w * 32 + __ffs(cand) - 1) * G;
+                cand &= cand - 1;
+                const float v = s.smooth_interior(j);
+                if (!(v > v2 || (v == v2 && j < j2)) || !far_enough(j))
+                    continue;
+                if (v > v1 || (v == v1 && j < j1)) {
+                    v2 = v1;
+                    j2 = j1;
+                    v1 = v;
+                    j1 = j;
+                } else {
+                    v2 = v;
+                    j2 = j;
+                }
             }
-        });
+        }
         float cut_v = v2;
         int cut_j = j2;
         argmax_pair(g, cut_v, cut_j); // cut_j == m: every candidate was collected
@@ -591,8 +646,8 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         int bj = pass1 ? j1 : pass2 ? j2 : m;
         argmax_pair(g, bv, bj);
         if (bj == m && cut_j != m) {
-            // Every candidate below the cut-off, each lane its own indices (lane l
-            // takes l+1, l+1+G, ...: candidates cluster on the peaks, and interleaving
+            // Every candidate below the cut-off, each lane its own (its samples are
+            // 1+l, 1+l+G, ...: candidates cluster on the peaks, and interleaving
             // spreads them over the lanes).  A lane takes one step per loop turn -- a
             // candidate check or one step of a prominence walk (the walks of
             // prominent(), unrolled, sliding a window over the signal: one new sample
@@ -601,26 +656,28 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
             auto smooth3 = [](float a, float b, float c) {
                 return radd(radd(rmul(0.25f, a), rmul(0.5f, b)), rmul(0.25f, c));
             };
-            int j = 1 + int(g.lane);
-            auto advance = [&]() { j += G; };
+            int cw = -1;
+            unsigned cand = 0;
+            int j = m;
             int walk = 0; // 0: checking candidates, -1 / +1: walking left / right of j
             int w = 0;
             float h = 0.0f, wo = 0.0f, wi = 0.0f; // walk window: at(w), at(w -/+ 1 towards j)
             bool fresh = true;
             while (true) {
                 if (walk == 0) {
-                    if (j + 1 >= m)
+                    while (cand == 0 && cw + 1 < words)
+                        cand = bits[++cw * G];
+                    if (cand == 0)
                         break;
+                    j = 1 + int(g.lane) + (cw * 32 + __ffs(cand) - 1) * G;
+                    cand &= cand - 1;
                     const float v = s.smooth_interior(j);
-                    if (v > 0.0f && (v < cut_v || (v == cut_v && j > cut_j)) && (v > bv || (v == bv && j < bj)) &&
-                        may_be_prominent(pmin, smin, m, j, v, threshold) && v > s.smooth(j - 1) &&
-                        v >= s.smooth(j + 1) && far_enough(j)) {
+                    if ((v < cut_v || (v == cut_v && j > cut_j)) && (v > bv || (v == bv && j < bj)) &&
+                        may_be_prominent(pmin, smin, m, j, v, threshold) && far_enough(j)) {
                         walk = -1;
                         w = j - 1;
                         h = v;
                         fresh = true;
-                    } else {
-                        advance();
                     }
                     continue;
                 }
@@ -685,10 +742,8 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
                         fail = true;
                     }
                 }
-                if (fail) {
+                if (fail)
                     walk = 0;
-                    advance();
-                }
             }
             argmax_pair(g, bv, bj);
         }
@@ -721,8 +776,8 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
             }
         }
         const int valley = mi;
-        primary = find_peak<MODEL, G>(g, s, xs, first, 0, valley, true);
-        const PeakFeature secondary = find_peak<MODEL, G>(g, s, xs, second, valley, m - 1, true);
+        primary = find_peak<G>(g, s, xs, first, 0, valley, true);
+        const PeakFeature secondary = find_peak<G>(g, s, xs, second, valley, m - 1, true);
         if (!primary.valid || !secondary.valid || !(primary.center < secondary.center))
             return kGuessInsufficient;
         out[0] = primary.amplitude;

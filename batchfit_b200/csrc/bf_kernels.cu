@@ -44,7 +44,9 @@ template <int MODEL> __host__ __device__ inline int lm_group_words(int m, int la
 __host__ __device__ inline int guess_group_words(int m, int lanes, int v) {
     const int n1 = pow2_at_least(edge_count(m));
     const int sorted = n1 > lanes * v ? n1 : lanes * v;
-    return bank_staggered(round_up(m, 4) + 2 * sorted, lanes); // y row + sorted edge runs
+    const int peaks = second_peak_words(m, lanes);
+    // y row + scratch: the sorted edge runs, later the second-peak search's arrays
+    return bank_staggered(round_up(m, 4) + (2 * sorted > peaks ? 2 * sorted : peaks), lanes);
 }
 __host__ __device__ inline int x_words(int m) { return round_up(m, 4); }
 
@@ -129,7 +131,7 @@ __global__ void __launch_bounds__(GuessShapeCfg<V>::threads, GuessShapeCfg<V>::m
         float syy;
         stage_fit_row(g, y, y_half, fit, m, vec_ok, ys, yfin, flat, syy);
         float p[P];
-        const int gs = initial_guess<MODEL, G, V>(g, cx, xs, ys, yfin, scratch, p);
+        const int gs = initial_guess<MODEL, G, V, true>(g, cx, xs, ys, yfin, scratch, p);
 #pragma unroll
         for (int k = 0; k < P; ++k)
             if (int(g.lane) == k)
