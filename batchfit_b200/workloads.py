@@ -118,6 +118,20 @@ def two_lorentzian_cube(n=262_144, m=1024, seed=3, chunk=32768):
                     {"noise_only": noise_only, "constant": constant})
 
 
+def noisy_doublets(m, n, seed):
+    """Two-Lorentzian rows, from resolved to merged, with noise strong enough that
+    most candidates of the second-peak search are noise maxima."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(-10, 10, m).astype(np.float32)
+    c = rng.uniform(-5, 5, n)[:, None]
+    w = np.exp(rng.uniform(np.log(0.2), np.log(2.0), n))[:, None]
+    a = rng.uniform(0.5, 4, n)[:, None]
+    c2 = c + rng.uniform(0.3, 4.0, n)[:, None] * w
+    y = a / (1 + ((x - c) / w) ** 2) + rng.uniform(0.1, 1.0, n)[:, None] * a / (1 + ((x - c2) / w) ** 2)
+    y = y + rng.uniform(0.005, 0.2, n)[:, None] * a * rng.normal(size=y.shape)
+    return x, y.astype(np.float32)
+
+
 MODEL_NAMES = ("gaussian", "lorentzian", "pseudo_voigt", "two_lorentzian")
 MIXED_BOUNDS = {
     "gaussian": ([0.0, -10.0, 1e-3], [np.inf, 10.0, 10.0]),

@@ -238,3 +238,21 @@ def test_autotune_table(bf):
         a, b = to_np(g), to_np(alone)
         for k in a:
             np.testing.assert_array_equal(a[k], b[k])
+
+
+@pytest.mark.parametrize("m", [1539, 6147, 10240])
+def test_batch_guess_equals_reference_guess(bf, oracle, m):
+    """The batch guess (x and y read in place, the shared-memory sort above
+    M = 5129) equals the reference float guess: a segment fitted from p0=None gives
+    the same bits as the same segment fitted from the oracle's guesses."""
+    x, y = W.noisy_doublets(m, 40, seed=m)
+    p0, status, _ = oracle.guess("port", "two_lorentzian", x, y, np.float32)
+    ok = status == 0
+    assert ok.sum() >= 10
+    bounds = W.MIXED_BOUNDS["two_lorentzian"]
+    bounds = (np.array(bounds[0], np.float32), np.array(bounds[1], np.float32))
+    base = dict(x=x, y=y[ok], model="two_lorentzian", bounds=bounds, group_lanes=32)
+    guessed, given = bf.fit_batch([base, dict(base, p0=p0[ok].astype(np.float32))])
+    a, b = to_np(guessed), to_np(given)
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=f"M={m} {k}")

@@ -98,3 +98,12 @@ def test_guess_paired_features(bf, oracle):
     xd = np.linspace(-5, 5, 2049).astype(np.float32)
     yd = two(xd, [3, -1.5, 0.7, 1, 1.5, 0.7, 0.4, 0]) + 0.3 * np.exp(-0.5 * ((xd + 2.25) / 0.015) ** 2)
     check_guess(bf, oracle, "two_lorentzian", xd, yd[None].astype(np.float32))
+
+
+# Samples per group lane (1 + lane + k*G, the second-peak candidate bits) at 32 and 33,
+# 96 and 97 for the 8-, 16- and 32-lane guess shapes, and the largest single-call M.
+@pytest.mark.parametrize("m", [258, 259, 1538, 1539, 3074, 3075, 5129])
+def test_guess_two_lorentzian_candidate_words(bf, oracle, m):
+    x, y = W.noisy_doublets(m, 96, seed=m)
+    s = check_guess(bf, oracle, "two_lorentzian", x, y)
+    assert np.count_nonzero(s == 0) >= 40
