@@ -11,6 +11,9 @@ larger than L2 (126 MB), so no L2 flush is needed between steps.
 * e2e       the same fits through the C ABI from pinned host buffers: host->device
             copies, kernels and device->host result copies inside each step.
 * accuracy  a 20,000-fit sample of the step's outputs against the float64 oracle.
+* mixed, serving, configs  (N=1) the uneven mixed-model batch, the served stream,
+            and the small-Lorentzian and two-Lorentzian-cube workloads with their
+            accuracy against the float64 oracle.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 
@@ -57,6 +60,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the uneven mixed-model batch section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream section")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the small-Lorentzian and two-Lorentzian-cube section")
     return ap.parse_args()
 
 
@@ -335,6 +340,81 @@ def mixed_section(ctx, dev):
                      "reference_float32_within_tol_fraction": round(within32 / max(definite, 1), 5),
                      "note": "fits the float64 oracle leaves at max_iterations are excluded (no definite status)"},
     }
+
+
+def configs_section(ctx, dev, steps=5, warmup=3):
+    """The other fixed-shape configurations, fitted on the GPU (device-resident,
+    p0=None, uncertainties, parity policy) and checked against the float64 oracle:
+    the reference's small CPU case (1,000 Lorentzians, M=129) and the two-Lorentzian
+    cube (262,144 spectra, M=1024; 5% pure-noise and 2% constant rows).  The
+    reference's own float32 path on the same sample is reported beside it."""
+    import ctypes as C
+
+    import torch
+
+    import batchfit_b200 as bf
+    from batchfit_b200 import _capi, accuracy, workloads
+    from oracle import pyoracle
+
+    impl = "ref" if pyoracle.ref_available() else "port"
+    dp = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    out = {}
+    for w, sample in ((workloads.lorentzian_small(), 1000), (workloads.two_lorentzian_cube(), 2000)):
+        n, m = w.y.shape
+        p = {"lorentzian": 3, "two_lorentzian": 8}[w.model]
+        opts = bf.solver_options(w.model, w.lower, w.upper, "parity")
+        x_d, y_d = torch.from_numpy(w.x).to(dev), torch.from_numpy(w.y).to(dev)
+        o = {"params": torch.empty((n, p), dtype=torch.float32, device=dev),
+             "status": torch.empty(n, dtype=torch.int32, device=dev),
+             "iters": torch.empty(n, dtype=torch.int32, device=dev),
+             "chi2": torch.empty(n, dtype=torch.float32, device=dev),
+             "cov": torch.empty((n, p, p), dtype=torch.float32, device=dev),
+             "se": torch.empty((n, p), dtype=torch.float32, device=dev),
+             "ustatus": torch.empty(n, dtype=torch.int32, device=dev)}
+        fa = _capi.FitArgs(workloads.MODEL_NAMES.index(w.model), n, m, dp(x_d), dp(y_d), None,
+                           _capi.BF_MEMORY_DEVICE, 1, 0, opts)
+        fo = _capi.FitOutputs(dp(o["params"]), dp(o["status"]), dp(o["iters"]), dp(o["chi2"]), dp(o["cov"]),
+                              dp(o["se"]), dp(o["ustatus"]))
+        for _ in range(warmup):
+            ctx.fit(fa, fo)
+        ms, split = [], {"guess_ms": [], "lm_ms": [], "covariance_ms": []}
+        for _ in range(steps):
+            ctx.fit(fa, fo)
+            t = ctx.timing()
+            ms.append(t.total_ms)
+            for k in split:
+                split[k].append(getattr(t, k))
+        res = {k: v.cpu().numpy() for k, v in o.items()}
+        k = min(sample, n)
+        ref = pyoracle.fit(impl, w.model, w.x, w.y[:k], None, w.lower, w.upper, np.float64, uncertainties=True)
+        r32 = pyoracle.fit(impl, w.model, w.x, w.y[:k], None, w.lower, w.upper, np.float32)
+        s = accuracy.summarize(w.model, w.x, w.y[:k], res["params"][:k], res["status"][:k], res["chi2"][:k],
+                               ref.params, ref.status, ref.chi2)
+        s32 = accuracy.summarize(w.model, w.x, w.y[:k], r32.params, r32.status, r32.chi2, ref.params, ref.status,
+                                 ref.chi2)
+        codes, counts = np.unique(res["status"], return_counts=True)
+        step_ms = statistics.median(ms)
+        out[w.name] = {
+            "fits": n, "points": m, "model": w.model, "fits_per_s": n / (step_ms * 1e-3),
+            "ms_per_step": round(step_ms, 3),
+            "kernels_ms": {k: round(statistics.median(v), 3) for k, v in split.items()},
+            "status_counts": {str(int(c)): int(v) for c, v in zip(codes, counts)},
+            "accuracy": {"oracle": f"float64 reference CPU path ({impl}) on the first {k} fits",
+                         "status_agreement": round(s["status_agreement"], 6),
+                         "within_tol_fraction": round(s["within_tol_fraction"], 6),
+                         "params_within_fraction": round(s["params_within_fraction"], 6),
+                         "chi2_within_fraction": round(s["chi2_within_fraction"], 6),
+                         "param_err_max": s["param_err_max"], "param_err_p999": s["param_err_p999"],
+                         "chi2_err_max": s["chi2_err_max"],
+                         "uncertainty_status_agreement": round(
+                             float((res["ustatus"][:k] == ref.uncertainty_status).mean()), 6),
+                         "reference_float32_within_tol_fraction": round(s32["within_tol_fraction"], 6),
+                         "reference_float32_status_agreement": round(s32["status_agreement"], 6),
+                         "param_tol": 1e-4, "chi2_tol": 1e-5},
+        }
+        del x_d, y_d, o
+        torch.cuda.empty_cache()
+    return out
 
 
 def serving_section(lib):
@@ -659,6 +739,7 @@ def run_cuda_arm(args, world, rank, local):
     # serving; the scaling runs repeat the plain workload per GPU).
     mixed = None if args.no_mixed or world > 1 else mixed_section(ctx, dev)
     serving = None if args.no_serving or world > 1 else serving_section(lib)
+    configs = None if args.no_configs or world > 1 else configs_section(ctx, dev)
     lat = sorted(step_ms)
     line = {
         "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world, "steps": args.steps,
@@ -680,6 +761,7 @@ def run_cuda_arm(args, world, rank, local):
         "cpu_baseline": cpu,
         "mixed": mixed,
         "serving": serving,
+        "configs": configs,
         "peaks_measured": {"fp32_tflops": round(peaks.fp32_tflops, 2), "fp64_tflops": round(peaks.fp64_tflops, 2),
                            "mufu_ex2_gops": round(peaks.mufu_ex2_gops, 1),
                            "mufu_rcp_gops": round(peaks.mufu_rcp_gops, 1)},
