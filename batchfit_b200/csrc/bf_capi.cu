@@ -70,8 +70,8 @@ int choose_lanes(int model, uint32_t m, int requested) {
         // Points per lane between ~8 and ~128 keeps the group reduction and the FP64
         // control amortised without starving the scheduler of independent fits.  The
         // two-Lorentzian pass carries 8 parameters and 36 J^T J sums per point, so its
-        // groups widen sooner (measured on B200: M=1024 runs 1.5x faster on 16 lanes
-        // than on 8).
+        // groups widen sooner (measured on B200 at M=1024: 16 lanes run 1.4x faster
+        // than 8 and 5% faster than 32).
         if (model == 3)
             lanes = m <= 128 ? 8 : m <= 2048 ? 16 : 32;
         else
