@@ -142,11 +142,13 @@ template <int MODEL, bool PRE = false> struct Signal {
         else
             return raw_at(j);
     }
-    __device__ __forceinline__ float raw_at(int j) const {
+    __device__ __forceinline__ float raw_at(int j) const { return raw(ys[j], xs[j]); }
+    // The signal of sample value yj at abscissa xj.
+    __device__ __forceinline__ float raw(float yj, float xj) const {
         if constexpr (Model<MODEL>::paired)
-            return rsub(ys[j], radd(level, rmul(slope, rsub(xs[j], left_x))));
+            return rsub(yj, radd(level, rmul(slope, rsub(xj, left_x))));
         else
-            return rsub(ys[j], level); // slope == 0: equal value (up to the sign of zero)
+            return rsub(yj, level); // slope == 0: equal value (up to the sign of zero)
     }
     // detail::smooth (initial_guess.hpp:32-36).
     __device__ __forceinline__ float smooth(int j) const {
@@ -527,13 +529,12 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         // a multiple of 4 floats, as is xs): overwrite it with the signal.
         const Signal<MODEL> raw{xs, ys, level, slope, xc.left_x, m};
         float4 *row = reinterpret_cast<float4 *>(const_cast<float *>(ys));
+        const float4 *xq = reinterpret_cast<const float4 *>(xs);
         for (int q = int(g.lane); 4 * q < m; q += G) {
-            float4 v;
-            v.x = raw.raw_at(4 * q);
-            v.y = raw.raw_at(4 * q + 1);
-            v.z = raw.raw_at(4 * q + 2);
-            v.w = raw.raw_at(4 * q + 3);
-            row[q] = v;
+            const float4 yv = row[q];
+            const float4 xv = paired ? xq[q] : yv; // x matters only with a slope
+            row[q] = make_float4(raw.raw(yv.x, xv.x), raw.raw(yv.y, xv.y), raw.raw(yv.z, xv.z),
+                                 raw.raw(yv.w, xv.w));
         }
         g.sync();
     }
