@@ -16,7 +16,11 @@ constexpr int kLmSlotDoubles = 2 * Layout<kTwoLorentzian>::K;
 constexpr int kLmWarpDoubles = 4 * kLmSlotDoubles;
 constexpr int kGuessWarpFloats = 2 * kBatchMaxSortWidth;
 constexpr int kGuessSmem = kBatchWarps * kGuessWarpFloats * int(sizeof(float));
-constexpr int kLmSmem = kBatchWarps * kLmWarpDoubles * int(sizeof(double));
+// The LM kernel runs 128-thread CTAs, 3 per SM: its two-Lorentzian classes need
+// 168 registers (at 128 a thread they spill several KB of state).
+constexpr int kBatchLmBlock = 128;
+constexpr int kBatchLmMinBlocks = 3;
+constexpr int kLmSmem = kBatchLmBlock / 32 * kLmWarpDoubles * int(sizeof(double));
 
 // Claim the next item of a class for a group: lane 0 takes a ticket, all lanes
 // get it.  False when the class is drained.

@@ -148,7 +148,7 @@ __device__ __forceinline__ void lm_class(const BatchArgs &b, const WorkClass &cl
     }
 }
 
-__global__ void __launch_bounds__(kBatchBlock, kBatchMinBlocks) batch_lm_kernel(BatchArgs b) {
+__global__ void __launch_bounds__(kBatchLmBlock, kBatchLmMinBlocks) batch_lm_kernel(BatchArgs b) {
     extern __shared__ __align__(16) double lm_smem[];
     double *warp_state = lm_smem + (threadIdx.x / 32) * kLmWarpDoubles;
     const int classes = b.hdr->lm_classes;
@@ -271,7 +271,7 @@ cudaError_t grids_for(int sms, Grids &out) {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(batch_lm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kLmSmem);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_lm, batch_lm_kernel, kBatchBlock, kLmSmem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_lm, batch_lm_kernel, kBatchLmBlock, kLmSmem);
     if (e != cudaSuccess)
         return e;
     Grids g;
@@ -332,7 +332,7 @@ cudaError_t launch_batch_pipeline(const BatchArgs &b, int sms, cudaStream_t stre
     launch_batch_guess(b, grids.guess, stream);
     if (guessed && (e = cudaEventRecord(guessed, stream)) != cudaSuccess)
         return e;
-    batch_lm_kernel<<<grids.lm, kBatchBlock, kLmSmem, stream>>>(b);
+    batch_lm_kernel<<<grids.lm, kBatchLmBlock, kLmSmem, stream>>>(b);
     if (fitted && (e = cudaEventRecord(fitted, stream)) != cudaSuccess)
         return e;
     batch_covariance_kernel<<<sms * 8, 128, 0, stream>>>(b);
