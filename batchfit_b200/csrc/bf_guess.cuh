@@ -682,66 +682,45 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
                     }
                     continue;
                 }
+                // One step of the walk in direction `walk` (both directions share this
+                // code, so the lanes of a warp do not split three ways).  The window
+                // keeps wo = at(w) and wi = at(w - walk); smoothing sums s[w-1],
+                // s[w], s[w+1] in that order, as detail::smooth does.
                 bool fail = false, clear = false;
-                if (walk < 0) {
-                    if (w < 0) {
-                        fail = true;
-                    } else if ((w & (kWalkBlock - 1)) == kWalkBlock - 1 && bmax[w / kWalkBlock] <= h) {
-                        clear = rsub(h, bmin[w / kWalkBlock]) > threshold;
-                        w -= kWalkBlock;
-                        fresh = true;
-                    } else {
-                        if (fresh) {
-                            wo = s.at(w);
-                            wi = s.at(w + 1);
-                            fresh = false;
-                        }
-                        float outer = 0.0f, v = wo;
-                        if (w > 0) {
-                            outer = s.at(w - 1);
-                            v = smooth3(outer, wo, wi);
-                        }
-                        fail = v > h;
-                        clear = !fail && rsub(h, v) > threshold;
-                        wi = wo;
-                        wo = outer;
-                        --w;
+                const int edge = walk < 0 ? 0 : m - 1; // no smoothing at the ends
+                if (walk < 0 ? w < 0 : w >= m) {
+                    fail = true;
+                } else if ((w & (kWalkBlock - 1)) == (walk < 0 ? kWalkBlock - 1 : 0) && bmax[w / kWalkBlock] <= h) {
+                    clear = rsub(h, bmin[w / kWalkBlock]) > threshold;
+                    w += walk * kWalkBlock;
+                    fresh = true;
+                } else {
+                    if (fresh) {
+                        wo = s.at(w);
+                        wi = s.at(w - walk);
+                        fresh = false;
                     }
-                    if (clear) { // left side clears: walk right
+                    float outer = 0.0f, v = wo;
+                    if (w != edge) {
+                        outer = s.at(w + walk);
+                        v = walk < 0 ? smooth3(outer, wo, wi) : smooth3(wi, wo, outer);
+                    }
+                    fail = v > h;
+                    clear = !fail && rsub(h, v) > threshold;
+                    wi = wo;
+                    wo = outer;
+                    w += walk;
+                }
+                if (clear) {
+                    if (walk < 0) { // left side clears: walk right
                         walk = 1;
                         w = j + 1;
                         fresh = true;
                         continue;
                     }
-                } else {
-                    if (w >= m) {
-                        fail = true;
-                    } else if ((w & (kWalkBlock - 1)) == 0 && bmax[w / kWalkBlock] <= h) {
-                        clear = rsub(h, bmin[w / kWalkBlock]) > threshold;
-                        w += kWalkBlock;
-                        fresh = true;
-                    } else {
-                        if (fresh) {
-                            wo = s.at(w);
-                            wi = s.at(w - 1);
-                            fresh = false;
-                        }
-                        float outer = 0.0f, v = wo;
-                        if (w < m - 1) {
-                            outer = s.at(w + 1);
-                            v = smooth3(wi, wo, outer);
-                        }
-                        fail = v > h;
-                        clear = !fail && rsub(h, v) > threshold;
-                        wi = wo;
-                        wo = outer;
-                        ++w;
-                    }
-                    if (clear) { // both sides clear: the lane's best so far
-                        bv = h;
-                        bj = j;
-                        fail = true;
-                    }
+                    bv = h; // both sides clear: the lane's best so far
+                    bj = j;
+                    fail = true;
                 }
                 if (fail)
                     walk = 0;
