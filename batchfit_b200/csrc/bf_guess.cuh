@@ -105,23 +105,24 @@ template <int G, int V> __device__ __forceinline__ void reg_merge(const Group<G>
         reg_stage<G, V>(g, v, N, j, true);
 }
 
-// k-th smallest (0-based) of the union of sorted a[0..na) and b[0..nb): a
-// merge-path binary search for how many of the k+1 smallest come from a.
-__device__ __forceinline__ float kth_of_two(const float *a, int na, const float *b, int nb, int k) {
-    int lo = k + 1 - nb > 0 ? k + 1 - nb : 0;
-    int hi = k + 1 < na ? k + 1 : na;
+// Median of the union of sorted a[0..n) and b[0..n) (2n values, an even count):
+// the midpoint of its n-1-th and n-th smallest.  One merge-path search splits off
+// the n smallest (i from a, n-i from b); the n-1-th is the larger of the last ones
+// taken, the n-th the smaller of the next ones.
+__device__ __forceinline__ float union_median(const float *a, const float *b, int n) {
+    int lo = 0, hi = n;
     while (lo < hi) {
         const int i = (lo + hi) >> 1;
-        const int j = k + 1 - i;
-        if (a[i] < b[j - 1])
+        if (a[i] < b[n - 1 - i])
             lo = i + 1;
         else
             hi = i;
     }
-    const int j = k + 1 - lo;
-    const float va = lo > 0 ? a[lo - 1] : -__int_as_float(0x7f800000);
-    const float vb = j > 0 ? b[j - 1] : -__int_as_float(0x7f800000);
-    return fmaxf(va, vb);
+    const float inf = __int_as_float(0x7f800000);
+    const int j = n - lo;
+    const float last = fmaxf(lo > 0 ? a[lo - 1] : -inf, j > 0 ? b[j - 1] : -inf);
+    const float next = fminf(lo < n ? a[lo] : inf, j < n ? b[j] : inf);
+    return midpoint_rn(last, next);
 }
 
 // detail::median on sorted values (initial_guess.hpp:25-30).
@@ -456,8 +457,7 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         g.sync();
         left_level = sorted_median(scratch, count);
         right_level = sorted_median(scratch + N, count);
-        baseline = midpoint_rn(kth_of_two(scratch, count, scratch + N, count, count - 1),
-                               kth_of_two(scratch, count, scratch + N, count, count));
+        baseline = union_median(scratch, scratch + N, count);
         slope = paired ? rdiv(rsub(right_level, left_level), rsub(xc.right_x, xc.left_x)) : 0.0f;
         level = paired ? left_level : baseline;
         g.sync();
@@ -477,8 +477,7 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
             scratch[N + int(g.lane) * V + i] = rv[i];
         }
         g.sync();
-        noise_median = midpoint_rn(kth_of_two(scratch, count, scratch + N, count, count - 1),
-                                   kth_of_two(scratch, count, scratch + N, count, count));
+        noise_median = union_median(scratch, scratch + N, count);
         g.sync();
     } else {
         // Edge medians (initial_guess.hpp:142-150) with shared-memory sorts.
