@@ -369,8 +369,12 @@ static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t strea
     int grid = 0, per_sm = 0;
     constexpr int kThreads = LmShape<MODEL>::threads;
     cudaError_t e = grid_for(lm_kernel<MODEL, G>, kThreads, smem, a.n, kThreads / G, sms, grid, per_sm);
-    if (e != cudaSuccess)
-        return e;
+    if (e != cudaSuccess || a.n == 0) {
+        // No fits: setting the attributes above has loaded the LM kernel; load the
+        // covariance kernel the same way and launch nothing.
+        cudaFuncAttributes attr;
+        return e != cudaSuccess ? e : cudaFuncGetAttributes(&attr, covariance_kernel<MODEL>);
+    }
     lm_kernel<MODEL, G><<<grid, kThreads, smem, stream>>>(a);
     if (info)
         *info = LaunchInfo{grid, kThreads, smem, per_sm, G};
@@ -390,8 +394,8 @@ static cudaError_t launch_guess_typed(const float *x, const float *y, long long 
     int grid = 0, per_sm = 0;
     constexpr int kThreads = GuessShapeCfg<V>::threads;
     cudaError_t e = grid_for(guess_kernel<MODEL, G, V>, kThreads, smem, n, kThreads / G, sms, grid, per_sm);
-    if (e != cudaSuccess)
-        return e;
+    if (e != cudaSuccess || n == 0)
+        return e; // no fits: the kernel is loaded (its attributes set), nothing launched
     guess_kernel<MODEL, G, V><<<grid, kThreads, smem, stream>>>(x, y, n, m, guesses, status, y_half);
     return cudaGetLastError();
 }

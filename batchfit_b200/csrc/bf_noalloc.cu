@@ -15,7 +15,6 @@
 #include "batchfit_cuda.h"
 #include "bf_kernels.h"
 
-#include <mutex>
 #include <string>
 
 namespace bf {
@@ -34,29 +33,18 @@ constexpr size_t kCounterBytes = 256; // the work counter, padded to the guess b
 // Layout: [0, 8) LM work counter; [256, end) guesses[N*P] when p0 is NULL.
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-unsigned char *g_scratch_address[kMaxDevices] = {};
-
-// The device address of the scratch array on the current device.  The host-side
-// symbol is only a stand-in, so it is resolved once per device with that device
-// current; the first call on a device does this.
-int scratch_on_current_device(unsigned char **out) {
-    int device = 0;
-    cudaError_t e = cudaGetDevice(&device);
+// The device address of the scratch array in the calling thread's current CUDA
+// context.  In host code the array's name is only a stand-in, not a device
+// address.  The address belongs to a context, not to a device (a caller may run
+// in a context of its own, or after cudaDeviceReset), so it is looked up on every
+// call; the lookup reads the runtime's module table and allocates nothing.  The
+// first lookup in a context loads this file's module, which places the array.
+int scratch_in_current_context(unsigned char **out) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess)
-        return bf::host::report_cuda(e, "cudaGetDevice");
-    if (device < 0 || device >= kMaxDevices)
-        return bf::host::report(BF_ERR_INVALID_ARGUMENT, "device index beyond the no-allocation table");
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_address[device]) {
-        void *ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess)
-            return bf::host::report_cuda(e, "cudaGetSymbolAddress(no-allocation scratch)");
-        g_scratch_address[device] = static_cast<unsigned char *>(ptr);
-    }
-    *out = g_scratch_address[device];
+        return bf::host::report_cuda(e, "cudaGetSymbolAddress(no-allocation scratch)");
+    *out = static_cast<unsigned char *>(ptr);
     return BF_OK;
 }
 
@@ -80,17 +68,15 @@ int bf_cuda_fit_noalloc(const bf_fit_args *args, const bf_fit_outputs *out, void
     if (args->memory != BF_MEMORY_DEVICE)
         return bf::host::report(BF_ERR_INVALID_ARGUMENT, "bf_cuda_fit_noalloc takes device memory only");
     if (args->y_format != BF_Y_FLOAT32)
-        return bf::host::report(BF_ERR_INVALID_ARGUMENT, "bf_cuda_fit_noalloc takes float32 y");
+        return bf::host::report(BF_ERR_INVALID_ARGUMENT, "bf_cuda_fit_noalloc takes float32 y (BF_Y_FLOAT32)");
     if (!args->p0 && args->n > max_guessed_fits(args->model))
         return bf::host::report(
             BF_ERR_INVALID_ARGUMENT,
             "bf_cuda_fit_noalloc: N=" + std::to_string(args->n) + " fits without p0 exceed the " +
                 std::to_string(max_guessed_fits(args->model)) +
                 " whose guesses fit the 4 MiB no-allocation scratch; pass p0 or split the batch");
-    if (args->n == 0)
-        return BF_OK;
     unsigned char *scratch = nullptr;
-    rc = scratch_on_current_device(&scratch);
+    rc = scratch_in_current_context(&scratch);
     if (rc != BF_OK)
         return rc;
     int device = 0, sms = 0;
@@ -103,6 +89,16 @@ int bf_cuda_fit_noalloc(const bf_fit_args *args, const bf_fit_outputs *out, void
     auto *counter = reinterpret_cast<unsigned long long *>(scratch);
     float *guesses = reinterpret_cast<float *>(scratch + kCounterBytes);
     const float *p0 = args->p0;
+    if (args->n == 0) {
+        // A warm-up: the scratch is placed and the kernels of (model, M, lanes) are
+        // loaded on this device; nothing is launched.
+        bf::FitArgs a = base;
+        a.n = 0;
+        e = bf::launch_guess(args->model, nullptr, nullptr, 0, int(args->m), nullptr, nullptr, sms, st);
+        if (e == cudaSuccess)
+            e = bf::launch_fit(args->model, lanes, a, sms, st, nullptr);
+        return e == cudaSuccess ? BF_OK : bf::host::report_cuda(e, "loading the fit kernels");
+    }
     if (!p0) {
         e = bf::launch_guess(args->model, args->x, args->y, (long long)args->n, int(args->m), guesses,
                              nullptr, sms, st);

@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("cuda", "reference"), default="cuda")
     ap.add_argument("--fits", type=int, default=1_000_000, help="fits per GPU per step")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    ap.add_argument("--cpu-seconds", type=float, default=9.0, help="CPU-baseline sample budget per precision")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the uneven mixed-model batch section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream section")
@@ -158,7 +158,7 @@ class ClockSampler:
                 "samples": len(sms)}
 
 
-HBM_FALLBACK_GBS = 6650.0  # an earlier copy-bandwidth measurement on this pool's B200s
+HBM_FALLBACK_GBS = 6650.0  # an earlier copy-bandwidth measurement on a B200
 
 
 def measured_peaks():
@@ -180,7 +180,10 @@ def hbm_peak():
 # ------------------------------------------------------------- CPU legs --
 def cpu_reference_rate(w, seconds_budget, dtype=np.float32):
     """The reference's own CPU path (oracle/_ref: guesses + cpu::fit_batch with
-    uncertainties) on all host threads, over a bounded sample of the workload."""
+    uncertainties) on all host threads, over a bounded sample of the workload.
+    Returns the rate with the data-only guesses included (what one fit call costs)
+    and, for the compiled reference, the rate of fit_batch alone (guesses excluded,
+    as the reference's own CPU timings are taken) and of the guesses alone."""
     from oracle import pyoracle
 
     if pyoracle.ref_available():
@@ -196,15 +199,19 @@ def cpu_reference_rate(w, seconds_budget, dtype=np.float32):
     run(n)  # warm-up and size probe
     per_fit = (time.perf_counter() - t0) / n
     n = int(min(w.y.shape[0], max(n, seconds_budget / 3 / max(per_fit, 1e-9))))
-    times = []
+    runs = []
     for _ in range(3):
         t0 = time.perf_counter()
-        run(n)
-        times.append(time.perf_counter() - t0)
-    sec = statistics.median(times)
-    return {"value": n / sec, "unit": "fits/s", "cores": cores, "kind": kind,
-            "sample": f"{n} fits of the same workload ({np.dtype(dtype).name} reference path incl. data-only guesses "
-                      f"and covariance), median of 3 after a warm-up"}
+        out = run(n)
+        runs.append((time.perf_counter() - t0, out.guess_seconds, out.fit_seconds))
+    sec, guess_s, fit_s = sorted(runs)[1]  # the median call
+    res = {"value": n / sec, "unit": "fits/s", "cores": cores, "kind": kind,
+           "sample": f"{n} fits of the same workload ({np.dtype(dtype).name} reference path incl. data-only guesses "
+                     f"and covariance), median of 3 after a warm-up"}
+    if kind == "reference" and fit_s > 0:
+        res["fit_only_value"] = n / fit_s
+        res["guess_only_value"] = n / guess_s if guess_s > 0 else None
+    return res
 
 
 def accuracy_sample(w, res_np, n=20000):
@@ -733,6 +740,16 @@ def run_cuda_arm(args, world, rank, local):
     cpu = None
     if not args.no_cpu_baseline:
         cpu = cpu_reference_rate(w, args.cpu_seconds)
+        # The float64 reference beside it (same inputs promoted), and the rates with
+        # the data-only guesses excluded, as the reference's CPU timings are taken.
+        c64 = cpu_reference_rate(w, args.cpu_seconds, np.float64)
+        cpu["value_f64"] = c64["value"]
+        cpu["sample_f64"] = c64["sample"]
+        for key in ("fit_only_value", "guess_only_value"):
+            if key in cpu:
+                cpu[key + "_f32"] = cpu.pop(key)
+            if key in c64:
+                cpu[key + "_f64"] = c64[key]
     del y_d, out_d
     torch.cuda.empty_cache()
     # The mixed-batch and serving sections run at N=1 only (one GPU's batching and

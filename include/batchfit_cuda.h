@@ -310,24 +310,32 @@ typedef struct bf_physical_outputs {
 } bf_physical_outputs;
 int bf_cuda_fit_physical(bf_cuda_context *ctx, const bf_physical_args *args, const bf_physical_outputs *out);
 
-/* A fit that allocates nothing.  No counterpart in the reference.
+/* A fit that needs no allocation of its own.  No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: a host whose memory pool already owns
  * the whole device, a real-time pipeline that reserves every buffer up front and
  * forbids allocation while it runs, or a library callback that may only enqueue
  * work on a stream it was given.  Every pointer in `args` and `out` is device
- * memory of the current device (args->memory must be BF_MEMORY_DEVICE); the work
- * is enqueued on `stream` (a cudaStream_t; NULL = the default stream) and the call
- * returns without waiting -- synchronise the stream before reading the outputs.
+ * memory of the current device (args->memory must be BF_MEMORY_DEVICE) and y is
+ * float32 (args->y_format must be BF_Y_FLOAT32); anything else is rejected with
+ * BF_ERR_INVALID_ARGUMENT.  The work is enqueued on `stream` (a cudaStream_t;
+ * NULL = the default stream) and the call returns without waiting -- synchronise
+ * the stream before reading the outputs.
  * The kernels' only scratch (the work counter and the data-only guesses) lives in
  * a 4 MiB static device array that every GPU loading this library holds until the
  * process exits.  With p0 == NULL, N is limited to the guesses that fit it --
  * 349,504 fits for P=3, 262,128 for P=4, 131,064 for P=8 -- and larger N is
- * rejected with BF_ERR_INVALID_ARGUMENT; with p0 given, N is not limited.  The
- * first call on a device resolves the array's device address (once per device)
- * and should come before any stream capture.  All calls share the array: calls
- * whose work overlaps on the GPU race, so serialise them (one stream, or wait
- * between calls).  No context is needed. */
+ * rejected with BF_ERR_INVALID_ARGUMENT; with p0 given, N is not limited.
+ * Every call looks up the array's device address in the calling thread's current
+ * context (a host-side lookup that allocates nothing).  The first call in a context
+ * loads the library's module and kernels, which places the array and the kernel
+ * code in device memory: make that first call -- a call with N == 0 loads
+ * everything for its model and M and launches nothing -- before a pool reserves
+ * the whole device, or set CUDA_MODULE_LOADING=EAGER; and make it before any
+ * stream capture.  All calls share the array and it keeps the last call's
+ * contents (the work counter is cleared by every call): calls whose work overlaps
+ * on the GPU race, so serialise them (one stream, or wait between calls).  No
+ * context is needed. */
 int bf_cuda_fit_noalloc(const bf_fit_args *args, const bf_fit_outputs *out, void *stream);
 
 /* Roofline denominators measured on the context's device: dependent-chain

@@ -109,7 +109,7 @@ def load_ref():
     global _ref
     if _ref is None:
         if not ref_available():
-            raise RuntimeError("reference build absent: run `make -C oracle ref` where the reference tree exists")
+            raise RuntimeError("reference build absent: run `make -C oracle ref REFERENCE=<batchfit tree>`")
         lib = C.CDLL(REF_PATH)
         vp, sz = C.c_void_p, C.c_size_t
         lib.bfref_fit.argtypes = [C.c_int, C.c_int, sz, sz, vp, vp, vp, vp, vp, C.POINTER(Options), C.c_int,

@@ -1,6 +1,6 @@
 """Regenerate the golden fixtures in this directory from the reference itself.
 
-    make -C oracle            # builds oracle/_ref/libbatchfit_ref.so from the reference sources
+    make -C oracle REFERENCE=<batchfit tree>   # builds oracle/_ref/libbatchfit_ref.so from the reference sources
     python tests/golden/make_golden.py
 
 Each fixture holds seeded float32 inputs and the reference's own outputs
@@ -45,7 +45,7 @@ def cases():
 
 def main():
     if not O.ref_available():
-        raise SystemExit("build the reference first: make -C oracle")
+        raise SystemExit("build the reference first: make -C oracle REFERENCE=<batchfit tree>")
     for name, model, x, y, lo, hi in cases():
         out = {"model": np.array(model), "x": x, "lower": lo, "upper": hi}
         if name == "lorentzian_small":

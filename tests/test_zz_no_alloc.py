@@ -1,91 +1,49 @@
 """bf_cuda_fit_noalloc: the fit entry point for callers that cannot allocate GPU
 memory (a host whose memory pool already owns the device, a real-time pipeline
 that forbids allocation while it runs, a callback that may only enqueue work on a
-stream it was given).  Its scratch lives in a fixed static device array, so this
-test checks, through the C ABI, that its results equal bf_cuda_fit's on the same
-device buffers, on two calls in a row (the shared scratch is reused and its work
-counter cleared), and that sizes beyond the array are rejected.
+stream it was given).  Its scratch lives in a fixed static device array, so these
+tests check, through the C ABI, that its results equal bf_cuda_fit's on the same
+device buffers bit for bit (both launch the same kernels with the same lanes per
+fit), on two calls in a row (the shared scratch is reused and its work counter
+cleared), and that sizes beyond the array and non-float32 y are rejected.
+
+The comparison runs in this process, after whatever ran before it, and in a fresh
+child process whose first library call is the no-allocation entry point (no
+bf_cuda_context exists there when it runs).  The shared body is
+tests/noalloc_check.py.
 
 Named to be collected last: a run that stops at the first failure has already run
-every other test.  It also passes alone in a fresh process."""
+every other test."""
 
 import ctypes as C
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
 
-from batchfit_b200 import workloads as W
-
 pytestmark = pytest.mark.gpu
 
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
 
-def _device_outputs(torch, n, p, dev):
-    return {"params": torch.empty((n, p), dtype=torch.float32, device=dev),
-            "status": torch.empty(n, dtype=torch.int32, device=dev),
-            "iterations": torch.empty(n, dtype=torch.int32, device=dev),
-            "chi2": torch.empty(n, dtype=torch.float32, device=dev),
-            "cov": torch.empty((n, p, p), dtype=torch.float32, device=dev),
-            "se": torch.empty((n, p), dtype=torch.float32, device=dev),
-            "ustatus": torch.empty(n, dtype=torch.int32, device=dev)}
-
-
-def _outs(capi, o):
-    dp = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
-    return capi.FitOutputs(dp(o["params"]), dp(o["status"]), dp(o["iterations"]), dp(o["chi2"]), dp(o["cov"]),
-                           dp(o["se"]), dp(o["ustatus"]))
-
-
-def _as_numpy(o):
-    return {k: v.cpu().numpy() for k, v in o.items()}
-
-
-def _assert_same(a, b):
-    # The tolerance of the fit parity tests; identical kernels give identical bits.
-    for key in ("status", "iterations", "ustatus"):
-        np.testing.assert_array_equal(a[key], b[key], err_msg=key)
-    for key in ("params", "chi2", "cov", "se"):
-        np.testing.assert_allclose(a[key], b[key], rtol=2e-4, atol=2e-4, err_msg=key)
+import noalloc_check  # noqa: E402
 
 
 @pytest.mark.parametrize("with_p0", [False, True])
-def test_noalloc_matches_fit_on_two_calls(bf, with_p0):
-    import torch
-
-    from batchfit_b200 import _capi
-
-    lib = _capi.load()
-    dev = torch.device("cuda", 0)
-    w = W.pseudo_voigt_plain(n=20_000, seed=21)
-    n, p = w.y.shape[0], 4
-    x = torch.from_numpy(w.x).to(dev)
-    y = torch.from_numpy(w.y).to(dev)
-    p0 = None
-    if with_p0:
-        guesses, _ = bf.guess(w.x, w.y, w.model)
-        fallback = np.array([2, 0, 1.7, 0.5], np.float32)
-        guesses[~np.isfinite(guesses).all(axis=1)] = fallback
-        p0 = torch.from_numpy(guesses).to(dev)
-    opts = bf.solver_options(w.model, w.lower, w.upper, "parity")
-    dp = lambda t: None if t is None else C.c_void_p(t.data_ptr())  # noqa: E731
-    args = _capi.FitArgs(2, n, w.x.size, dp(x), dp(y), dp(p0), _capi.BF_MEMORY_DEVICE, 1, 0, opts)
-
-    # The existing entry point on the same device buffers.
-    ref = _device_outputs(torch, n, p, dev)
-    torch.cuda.synchronize()
-    bf.context(0).fit(args, _outs(_capi, ref))
-    ref = _as_numpy(ref)
-
-    stream = torch.cuda.current_stream(dev)
-    for _ in range(2):
-        got = _device_outputs(torch, n, p, dev)
-        torch.cuda.synchronize()
-        rc = lib.bf_cuda_fit_noalloc(C.byref(args), C.byref(_outs(_capi, got)), C.c_void_p(stream.cuda_stream))
-        assert rc == _capi.BF_OK, _capi.last_error()
-        stream.synchronize()
-        _assert_same(_as_numpy(got), ref)
+def test_noalloc_matches_fit_bitwise_on_two_calls(bf, with_p0):
+    assert noalloc_check.compare(with_p0, noalloc_first=False) == []
 
 
-def test_noalloc_rejects_sizes_beyond_its_scratch(bf):
+def test_noalloc_first_call_in_a_fresh_process(bf):
+    res = subprocess.run([sys.executable, os.path.join(HERE, "noalloc_check.py")], capture_output=True, text=True,
+                         timeout=600)
+    assert res.returncode == 0, res.stdout[-2000:] + res.stderr[-4000:]
+    assert "BITWISE_EQUAL" in res.stdout, res.stdout[-2000:]
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch_and_half_y(bf):
     import torch
 
     from batchfit_b200 import _capi
@@ -97,10 +55,13 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(bf):
     y = torch.zeros((n, m), device=dev)
     opts = bf.solver_options("pseudo_voigt", [-np.inf] * 4, [np.inf] * 4, "parity")
     dp = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    bufs = [torch.empty(16, dtype=torch.float32, device=dev) for _ in range(7)]
+    outs = _capi.FitOutputs(*(dp(b) for b in bufs))
     args = _capi.FitArgs(2, n, m, dp(x), dp(y), None, _capi.BF_MEMORY_DEVICE, 0, 0, opts)
-    o = _device_outputs(torch, 1, 4, dev)
-    rc = lib.bf_cuda_fit_noalloc(C.byref(args), C.byref(_outs(_capi, o)), None)
-    assert rc == _capi.BF_ERR_INVALID_ARGUMENT
+    assert lib.bf_cuda_fit_noalloc(C.byref(args), C.byref(outs), None) == _capi.BF_ERR_INVALID_ARGUMENT
     assert "4 MiB" in _capi.last_error() and "262128" in _capi.last_error()
     host = _capi.FitArgs(2, 4, m, dp(x), dp(y), None, _capi.BF_MEMORY_HOST, 0, 0, opts)
-    assert lib.bf_cuda_fit_noalloc(C.byref(host), C.byref(_outs(_capi, o)), None) == _capi.BF_ERR_INVALID_ARGUMENT
+    assert lib.bf_cuda_fit_noalloc(C.byref(host), C.byref(outs), None) == _capi.BF_ERR_INVALID_ARGUMENT
+    half = _capi.FitArgs(2, 4, m, dp(x), dp(y), None, _capi.BF_MEMORY_DEVICE, 0, 0, opts, _capi.BF_Y_FLOAT16)
+    assert lib.bf_cuda_fit_noalloc(C.byref(half), C.byref(outs), None) == _capi.BF_ERR_INVALID_ARGUMENT
+    assert "float32" in _capi.last_error()
