@@ -317,6 +317,16 @@ class _Ticket:
             _capi.check(-rc, "bf_server_poll")
         return rc == 1
 
+    def cancel(self) -> bool:
+        """Cancel the request if it has not been admitted yet (then ``result()``
+        raises concurrent.futures.CancelledError); False once it is admitted."""
+        if self._code is not None:
+            return False
+        rc = self._server._lib.bf_server_cancel(self._server._ptr, self._ticket)
+        if rc < 0:
+            _capi.check(-rc, "bf_server_cancel")
+        return rc == 1
+
     def result(self):
         if self._code is None:
             latency = C.c_double()
@@ -389,6 +399,11 @@ class Server:
             result = FitResult(params, status, iterations, chi2)
         self._live[ticket.value] = (x, y, p0, result)
         return _Ticket(self, ticket.value, result, None)
+
+    def _fail_allocations(self, count: int):
+        """Failure injection for tests: the next `count` admissions fail as if the
+        device allocation ran out of memory (on the host; no GPU fault)."""
+        _capi.check(self._lib.bf_server_fail_allocations(self._ptr, int(count)), "bf_server_fail_allocations")
 
     def stats(self) -> dict:
         st = _capi.ServerStats()

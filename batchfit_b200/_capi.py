@@ -6,6 +6,7 @@ the library is missing, loading raises RuntimeError naming the build command.
 
 from __future__ import annotations
 
+import concurrent.futures
 import ctypes as C
 import os
 import threading
@@ -19,6 +20,7 @@ BF_ERR_INVALID_ARGUMENT = 1
 BF_ERR_CUDA = 2
 BF_ERR_UNAVAILABLE = 3
 BF_ERR_BUSY = 4
+BF_ERR_CANCELLED = 5
 BF_MEMORY_HOST = 0
 BF_MEMORY_DEVICE = 1
 BF_POLICY_REFERENCE = 0
@@ -32,7 +34,8 @@ EXPORTS = (
     "bf_cuda_max_points", "bf_cuda_measure_peaks", "bf_cuda_fit_noalloc", "bf_cuda_fit_batch",
     "bf_cuda_batch_max_points", "bf_cuda_autotune", "bf_cuda_get_tuning", "bf_cuda_set_tuning",
     "bf_server_create", "bf_server_destroy", "bf_server_submit", "bf_server_poll", "bf_server_wait",
-    "bf_server_get_stats", "bf_cuda_fit_npy", "bf_npy_inspect", "bf_cuda_fit_physical",
+    "bf_server_get_stats", "bf_server_cancel", "bf_server_fail_allocations", "bf_cuda_fit_npy", "bf_npy_inspect",
+    "bf_cuda_fit_physical",
 )
 
 BF_Y_FLOAT32, BF_Y_FLOAT16 = 0, 1
@@ -193,6 +196,8 @@ def load():
         lib.bf_server_poll.argtypes = [vp, C.c_uint64]
         lib.bf_server_wait.argtypes = [vp, C.c_uint64, C.POINTER(C.c_double)]
         lib.bf_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
+        lib.bf_server_cancel.argtypes = [vp, C.c_uint64]
+        lib.bf_server_fail_allocations.argtypes = [vp, C.c_uint32]
         lib.bf_cuda_fit_npy.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(NpyOptions),
                                         C.POINTER(NpyStats)]
         lib.bf_cuda_fit_physical.argtypes = [vp, C.POINTER(PhysicalArgs), C.POINTER(PhysicalOutputs)]
@@ -216,6 +221,8 @@ def check(rc: int, what: str = "batchfit CUDA call"):
         raise ValueError(f"{what}: {message}")
     if rc == BF_ERR_UNAVAILABLE:
         raise RuntimeError(f"CUDA fitting is unavailable: {message}")
+    if rc == BF_ERR_CANCELLED:
+        raise concurrent.futures.CancelledError(f"{what}: {message}")
     raise RuntimeError(f"{what} failed ({rc}): {message}")
 
 

@@ -21,10 +21,10 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbatchfit_cuda.so")
 OBJ = os.path.join(HERE, "_build")
-SOURCES = ["bf_kernels.cu", "bf_capi.cu", "bf_noalloc.cu", "bf_batch.cu", "bf_batch_kernels.cu", "bf_batch_guess.cu",
+SOURCES = ["bf_kernels.cu", "bf_long.cu", "bf_capi.cu", "bf_noalloc.cu", "bf_batch.cu", "bf_batch_kernels.cu", "bf_batch_guess.cu",
            "bf_server.cu", "bf_npy.cu", "bf_coords.cu"]
 HEADERS = ["bf_args.h", "bf_batch.h", "bf_batch.cuh", "bf_context.h", "bf_device.cuh", "bf_guess.cuh", "bf_kernels.h",
-           "bf_lm.cuh", "bf_models.cuh"]
+           "bf_lm.cuh", "bf_models.cuh", "bf_xgrid.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]

@@ -64,7 +64,8 @@ namespace {
 
 constexpr int kSmemLimit = 227 * 1024;
 
-int choose_lanes(int model, uint32_t m, int requested) {
+// Lanes per fit of the group kernels (8, 16 or 32) for (model, M).
+int choose_group_lanes(int model, uint32_t m, int requested) {
     int lanes = requested;
     if (lanes != 8 && lanes != 16 && lanes != 32) {
         // Points per lane between ~8 and ~128 keeps the group reduction and the FP64
@@ -78,9 +79,18 @@ int choose_lanes(int model, uint32_t m, int requested) {
             lanes = m <= 1024 ? 8 : m <= 2048 ? 16 : 32;
     }
     // Fewer, wider groups per CTA when the per-group spectrum buffers do not fit.
-    while (lanes < 32 && bf::smem_bytes(model, lanes, int(m)) > kSmemLimit)
+    while (lanes < 32 && bf::group_smem_bytes(model, lanes, int(m)) > kSmemLimit)
         lanes *= 2;
     return lanes;
+}
+
+// Lanes per fit of a bf_cuda_fit call: a group width, or bf::kCtaLanes (one CTA per
+// fit) when asked for or when the spectrum does not fit the group layout.
+int choose_lanes(int model, uint32_t m, int requested) {
+    if (requested == bf::kCtaLanes)
+        return bf::kCtaLanes;
+    const int lanes = choose_group_lanes(model, m, requested);
+    return bf::group_smem_bytes(model, lanes, int(m)) > kSmemLimit ? bf::kCtaLanes : lanes;
 }
 
 bool options_valid(const bf_solver_options &o, int p) {
@@ -140,17 +150,24 @@ int validate(const bf_fit_args *args, const bf_fit_outputs *out, uint32_t limit 
     if (args->memory != BF_MEMORY_HOST && args->memory != BF_MEMORY_DEVICE)
         return fail(BF_ERR_INVALID_ARGUMENT, "memory must be BF_MEMORY_HOST or BF_MEMORY_DEVICE");
     if (limit == 0)
-        limit = uint32_t(bf::max_points(args->model));
+        limit = uint32_t(bf::kMaxPoints);
     if (args->m > limit)
         return fail(BF_ERR_INVALID_ARGUMENT,
                     "M=" + std::to_string(args->m) + " exceeds this backend's limit of " + std::to_string(limit));
     const int p = parameter_count(args->model);
     if (args->n > uint64_t(std::numeric_limits<int64_t>::max()) / (uint64_t(args->m) + uint64_t(p) * p))
         return fail(BF_ERR_INVALID_ARGUMENT, "N*M or N*P*P overflows 64-bit indexing");
-    if (args->group_lanes != 0 && args->group_lanes != 8 && args->group_lanes != 16 && args->group_lanes != 32)
-        return fail(BF_ERR_INVALID_ARGUMENT, "group_lanes must be 0, 8, 16 or 32");
+    if (args->group_lanes != 0 && args->group_lanes != 8 && args->group_lanes != 16 && args->group_lanes != 32 &&
+        args->group_lanes != bf::kCtaLanes)
+        return fail(BF_ERR_INVALID_ARGUMENT, "group_lanes must be 0, 8, 16, 32 or 128 (one CTA per fit)");
     if (args->y_format != BF_Y_FLOAT32 && args->y_format != BF_Y_FLOAT16)
         return fail(BF_ERR_INVALID_ARGUMENT, "y_format must be BF_Y_FLOAT32 or BF_Y_FLOAT16");
+    if (args->y_format == BF_Y_FLOAT16 &&
+        (choose_lanes(args->model, args->m, args->group_lanes) == bf::kCtaLanes ||
+         (!args->p0 && args->m > uint32_t(bf::group_guess_max_points()))))
+        return fail(BF_ERR_INVALID_ARGUMENT,
+                    "half-precision y (BF_Y_FLOAT16) is staged by the group kernels only: M=" +
+                        std::to_string(args->m) + " needs float32 y");
     if (args->n == 0)
         return BF_OK;
     if (!args->x || !args->y)
@@ -177,13 +194,18 @@ cudaEvent_t take_event(bf_cuda_context *ctx) {
 // guess when there are no initial values (into `guess_buf`), then the LM kernel.
 int launch_batch(bf_cuda_context *ctx, const bf_fit_args &in, const bf::FitArgs &base, int lanes, const float *x,
                  const float *y, const float *p0, float *guess_buf, int32_t *guess_status, bool guess_only,
-                 const bf_fit_outputs &dev_out, unsigned long long *counter, long long count, cudaStream_t st) {
+                 const bf_fit_outputs &dev_out, unsigned long long *counter, long long count, cudaStream_t st,
+                 bf::host::DeviceBuffer &scratch) {
     // Four events bracket the guess, LM and covariance kernels of this batch.
     KernelEvents ev{take_event(ctx), take_event(ctx), take_event(ctx), take_event(ctx)};
     BF_CUDA(cudaEventRecord(ev.start, st));
     if (!p0 || guess_only) {
+        const size_t scratch_bytes =
+            in.m > uint32_t(bf::group_guess_max_points()) ? bf::long_guess_scratch_bytes(int(in.m), ctx->sms) : 0;
+        if (scratch_bytes)
+            BF_CUDA(scratch.reserve(scratch_bytes));
         BF_CUDA(bf::launch_guess(in.model, x, y, count, int(in.m), guess_buf, guess_status, ctx->sms, st,
-                                 base.y_half));
+                                 base.y_half, scratch_bytes ? static_cast<float *>(scratch.ptr) : nullptr));
         ++ctx->launches;
         p0 = guess_buf;
     }
@@ -246,7 +268,7 @@ int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &o
         if (n > 0) {
             const int rc = launch_batch(ctx, in, base, lanes, in.x, in.y, in.p0, gbuf, gstat, guess_only != nullptr,
                                         out, static_cast<unsigned long long *>(s.counter.ptr), (long long)n,
-                                        ctx->stream[0]);
+                                        ctx->stream[0], s.scratch);
             if (rc != BF_OK)
                 return rc;
         }
@@ -305,7 +327,8 @@ int enqueue(bf_cuda_context *ctx, const bf_fit_args &in, const bf_fit_outputs &o
                                     static_cast<const float *>(s.y.ptr),
                                     has_p0 ? static_cast<const float *>(s.p0.ptr) : nullptr,
                                     static_cast<float *>(s.guess.ptr), nullptr, false, dev_out,
-                                    static_cast<unsigned long long *>(s.counter.ptr), (long long)count, st);
+                                    static_cast<unsigned long long *>(s.counter.ptr), (long long)count, st,
+                                    s.scratch);
         if (rc != BF_OK)
             return rc;
         auto d2h = [&](void *dst, const void *src, size_t bytes) {
@@ -378,7 +401,7 @@ int prepare_segment(const bf_fit_args *args, const bf_fit_outputs *out, uint32_t
     *base = make_args(*args, parameter_count(args->model));
     return BF_OK;
 }
-int default_lanes(int model, uint32_t m) { return choose_lanes(model, m, 0); }
+int default_lanes(int model, uint32_t m) { return choose_group_lanes(model, m, 0); }
 int report(int code, const std::string &message) { return fail(code, message); }
 int report_cuda(cudaError_t e, const char *what) { return cuda_fail(e, what); }
 } // namespace host
@@ -407,7 +430,7 @@ int bf_cuda_available(void) {
 uint32_t bf_cuda_max_points(int32_t model) {
     if (model < 0 || model > 3)
         return 0;
-    return uint32_t(bf::max_points(model));
+    return uint32_t(bf::kMaxPoints);
 }
 
 int bf_cuda_context_create(int device, bf_cuda_context **out) {
@@ -465,6 +488,7 @@ void bf_cuda_context_destroy(bf_cuda_context *ctx) {
         s.se.release();
         s.ustatus.release();
         s.counter.release();
+        s.scratch.release();
     }
     ctx->x.release();
     bf::host::release_batch_state(ctx->batch);

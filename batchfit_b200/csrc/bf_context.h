@@ -38,6 +38,7 @@ struct DeviceBuffer {
 // Device-side storage of one in-flight chunk.
 struct Slot {
     DeviceBuffer y, p0, guess, params, status, iterations, chi2, cov, se, ustatus, counter;
+    DeviceBuffer scratch; // long-spectrum guess scratch when it exceeds shared memory
 };
 
 constexpr int kSlots = 2;

@@ -13,6 +13,7 @@ namespace bf {
 // fit.  Several groups of a warp proceed independently (each has its own mask).
 template <int G> struct Group {
     static_assert(G == 8 || G == 16 || G == 32, "group size");
+    static constexpr int size = G;
     unsigned lane;  // 0..G-1
     unsigned base;  // first warp lane of this group
     unsigned mask;  // member lanes within the warp
@@ -38,6 +39,15 @@ template <int G> struct Group {
     }
     __device__ __forceinline__ bool any(bool p) const { return ballot(p) != 0u; }
     __device__ __forceinline__ bool all(bool p) const { return ballot(!p) == 0u; }
+};
+
+// A whole CTA of THREADS threads cooperating on one fit (the long-spectrum path):
+// the same members the per-fit control code uses from a Group.
+template <int THREADS> struct CtaGroup {
+    static constexpr int size = THREADS;
+    unsigned lane; // threadIdx.x
+    __device__ __forceinline__ CtaGroup() : lane(threadIdx.x) {}
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
 
 // ----------------------------------------------------- exactly rounded ops --
@@ -94,6 +104,25 @@ __device__ __forceinline__ float rcp_approx(float v) {
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
     return r;
 }
+
+// ------------------------------------------------- packed float32 pairs --
+// sm_100 f32x2 arithmetic: one instruction computes two IEEE float32 results, each
+// rounded to nearest exactly as the scalar operation would be.  The LM pass
+// evaluates two adjacent points per lane with these, halving its issue slots.
+__device__ __forceinline__ float2 splat2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<const unsigned long long *>(&a)),
+          "l"(*reinterpret_cast<const unsigned long long *>(&b)));
+    return *reinterpret_cast<const float2 *>(&d);
+}
+__device__ __forceinline__ float2 ex2_approx2(float2 v) { return make_float2(ex2_approx(v.x), ex2_approx(v.y)); }
+__device__ __forceinline__ float2 rcp_approx2(float2 v) { return make_float2(rcp_approx(v.x), rcp_approx(v.y)); }
 
 // --------------------------------------------------- compensated sums --
 // Knuth two-sum: s + e == a + b exactly.

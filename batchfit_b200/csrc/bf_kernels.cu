@@ -25,23 +25,26 @@ template <int V> struct GuessShapeCfg {
     static constexpr int threads = V > 0 && V <= 8 ? 128 : 256;
     static constexpr int min_blocks = V > 0 && V <= 8 ? 5 : 2;
 };
-// LM kernel CTA shape per model.  The 3- and 4-parameter passes fit in 102 registers
-// a thread: 128-thread CTAs, 5 per SM, give 20 warps per SM where 256-thread CTAs
-// fit only two (16 warps) -- measured 6-20% faster on B200.  The two-Lorentzian
+// LM kernel CTA shape per model.  The 3- and 4-parameter paired passes need 128
+// registers a thread: 128-thread CTAs, 4 per SM (16 warps; at 5 per SM, 96
+// registers, they spill and run 7% slower on B200).  The two-Lorentzian
 // state (8 parameters, 36 J^T J sums, an 8x8 FP64 Cholesky) spills heavily at 128
 // registers; 128-thread CTAs, 3 per SM, allow 168 (12 warps per SM, little
 // spilling) -- measured 5% faster on B200 than 256 threads, 2 per SM.
 template <int MODEL> struct LmShape {
     static constexpr int threads = 128;
-    static constexpr int min_blocks = MODEL == kTwoLorentzian ? 3 : 5;
+    static constexpr int min_blocks = MODEL == kTwoLorentzian ? 3 : 4;
 };
 
 // Per-group shared memory, in 4-byte words, padded so that consecutive groups of a
 // warp start G banks apart.
 __host__ __device__ inline int bank_staggered(int words, int lanes) { return round_up(words, 32) + (lanes % 32); }
 
+// The LM pass reads its row as 8-byte pairs, which a warp serves in two phases of 16
+// lanes: groups of 8 lanes start 16 banks apart so that the two groups of a phase
+// read disjoint banks (wider groups fill a phase alone).
 template <int MODEL> __host__ __device__ inline int lm_group_words(int m, int lanes) {
-    return bank_staggered(round_up(m, 4) + 4 * Layout<MODEL>::K, lanes); // y row + 2 FP64 state slots
+    return round_up(round_up(m, 4) + 4 * Layout<MODEL>::K, 32) + (2 * lanes) % 32; // y row + 2 FP64 state slots
 }
 __host__ __device__ inline int guess_group_words(int m, int lanes, int v) {
     const int n1 = pow2_at_least(edge_count(m));
@@ -198,19 +201,19 @@ __global__ void __launch_bounds__(LmShape<MODEL>::threads, LmShape<MODEL>::min_b
                 s.status = kInvalid;
                 s.iterations = 0;
                 s.chi2 = __longlong_as_double(0x7ff8000000000000ll);
-                write_fit<MODEL, G>(g, a, f, s);
+                write_fit<MODEL>(g, a, f, s);
             }
             if (fit < 0)
                 break;
         }
-        const bool pass_finite = lm_pass<MODEL, G>(g, xs, ys, m, s.t, state + (1 - s.cur) * Layout<MODEL>::K);
-        bool done = lm_after_pass<MODEL, G>(g, a, cx, flat, pass_finite, state, s);
+        const bool pass_finite = lm_pass<MODEL, G, true>(g, xs, ys, m, s.t, state + (1 - s.cur) * Layout<MODEL>::K);
+        bool done = lm_after_pass<MODEL>(g, a, cx, flat, pass_finite, state, s);
         if (!done)
             done = lm_plan<MODEL>(a, cx, double(syy), state, s);
         if (done) {
-            write_fit<MODEL, G>(g, a, fit, s);
+            write_fit<MODEL>(g, a, fit, s);
             if (a.uncertainties && s.status == kConverged)
-                write_information<MODEL, G>(g, a, fit, state + s.cur * Layout<MODEL>::K);
+                write_information<MODEL>(g, a, fit, state + s.cur * Layout<MODEL>::K);
             g.sync();
             fit = -1;
         }
@@ -363,26 +366,24 @@ template <class K> static cudaError_t grid_for(K kernel, int block, int smem, lo
 }
 
 template <int MODEL, int G>
-static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t stream, LaunchInfo *info,
-                                   cudaEvent_t lm_done) {
+static cudaError_t launch_lm_typed(const FitArgs &a, int sms, cudaStream_t stream, LaunchInfo *info) {
     const int smem = lm_smem_bytes<MODEL, G>(a.m);
     int grid = 0, per_sm = 0;
     constexpr int kThreads = LmShape<MODEL>::threads;
     cudaError_t e = grid_for(lm_kernel<MODEL, G>, kThreads, smem, a.n, kThreads / G, sms, grid, per_sm);
-    if (e != cudaSuccess || a.n == 0) {
-        // No fits: setting the attributes above has loaded the LM kernel; load the
-        // covariance kernel the same way and launch nothing.
-        cudaFuncAttributes attr;
-        return e != cudaSuccess ? e : cudaFuncGetAttributes(&attr, covariance_kernel<MODEL>);
-    }
+    if (e != cudaSuccess || a.n == 0)
+        return e; // no fits: setting the attributes above has loaded the kernel
     lm_kernel<MODEL, G><<<grid, kThreads, smem, stream>>>(a);
     if (info)
         *info = LaunchInfo{grid, kThreads, smem, per_sm, G};
-    e = cudaGetLastError();
-    if (e == cudaSuccess && lm_done)
-        e = cudaEventRecord(lm_done, stream);
-    if (e != cudaSuccess || !a.uncertainties || a.n == 0)
-        return e;
+    return cudaGetLastError();
+}
+
+template <int MODEL> static cudaError_t launch_covariance_typed(const FitArgs &a, cudaStream_t stream) {
+    if (a.n == 0) {
+        cudaFuncAttributes attr; // loads the kernel
+        return cudaFuncGetAttributes(&attr, covariance_kernel<MODEL>);
+    }
     covariance_kernel<MODEL><<<unsigned((a.n + kCovBlock - 1) / kCovBlock), kCovBlock, 0, stream>>>(a);
     return cudaGetLastError();
 }
@@ -419,11 +420,19 @@ __host__ __device__ inline GuessShape guess_shape(int m) {
 template <int MODEL>
 static cudaError_t launch_lm_model(const FitArgs &a, int lanes, int sms, cudaStream_t s, LaunchInfo *info,
                                    cudaEvent_t lm_done) {
+    cudaError_t e;
     switch (lanes) {
-    case 8: return launch_lm_typed<MODEL, 8>(a, sms, s, info, lm_done);
-    case 16: return launch_lm_typed<MODEL, 16>(a, sms, s, info, lm_done);
-    default: return launch_lm_typed<MODEL, 32>(a, sms, s, info, lm_done);
+    case 8: e = launch_lm_typed<MODEL, 8>(a, sms, s, info); break;
+    case 16: e = launch_lm_typed<MODEL, 16>(a, sms, s, info); break;
+    case 32: e = launch_lm_typed<MODEL, 32>(a, sms, s, info); break;
+    case kCtaLanes: e = launch_lm_cta(MODEL, a, sms, s, info); break;
+    default: return cudaErrorInvalidValue;
     }
+    if (e == cudaSuccess && lm_done)
+        e = cudaEventRecord(lm_done, s);
+    if (e != cudaSuccess || !a.uncertainties)
+        return e;
+    return launch_covariance_typed<MODEL>(a, s);
 }
 
 template <int MODEL>
@@ -454,7 +463,12 @@ cudaError_t launch_fit(int model, int lanes, const FitArgs &a, int sms, cudaStre
 }
 
 cudaError_t launch_guess(int model, const float *x, const float *y, long long n, int m, float *guesses,
-                         int32_t *status, int sms, cudaStream_t s, int y_half) {
+                         int32_t *status, int sms, cudaStream_t s, int y_half, float *gscratch) {
+    if (m > group_guess_max_points()) {
+        if (y_half)
+            return cudaErrorInvalidValue; // long spectra take float32 y
+        return launch_guess_long(model, x, y, n, m, guesses, status, sms, s, gscratch);
+    }
     switch (model) {
     case kGaussian: return launch_guess_model<kGaussian>(x, y, n, m, guesses, status, sms, s, y_half);
     case kLorentzian: return launch_guess_model<kLorentzian>(x, y, n, m, guesses, status, sms, s, y_half);
@@ -464,43 +478,54 @@ cudaError_t launch_guess(int model, const float *x, const float *y, long long n,
     }
 }
 
-int smem_bytes(int model, int lanes, int m) {
-    int lm = 0, gs = 0;
+int group_smem_bytes(int model, int lanes, int m) {
     switch (model * 100 + lanes) {
-    case 8: lm = lm_smem_bytes<0, 8>(m); break;
-    case 16: lm = lm_smem_bytes<0, 16>(m); break;
-    case 32: lm = lm_smem_bytes<0, 32>(m); break;
-    case 108: lm = lm_smem_bytes<1, 8>(m); break;
-    case 116: lm = lm_smem_bytes<1, 16>(m); break;
-    case 132: lm = lm_smem_bytes<1, 32>(m); break;
-    case 208: lm = lm_smem_bytes<2, 8>(m); break;
-    case 216: lm = lm_smem_bytes<2, 16>(m); break;
-    case 232: lm = lm_smem_bytes<2, 32>(m); break;
-    case 308: lm = lm_smem_bytes<3, 8>(m); break;
-    case 316: lm = lm_smem_bytes<3, 16>(m); break;
-    default: lm = lm_smem_bytes<3, 32>(m); break;
+    case 8: return lm_smem_bytes<0, 8>(m);
+    case 16: return lm_smem_bytes<0, 16>(m);
+    case 32: return lm_smem_bytes<0, 32>(m);
+    case 108: return lm_smem_bytes<1, 8>(m);
+    case 116: return lm_smem_bytes<1, 16>(m);
+    case 132: return lm_smem_bytes<1, 32>(m);
+    case 208: return lm_smem_bytes<2, 8>(m);
+    case 216: return lm_smem_bytes<2, 16>(m);
+    case 232: return lm_smem_bytes<2, 32>(m);
+    case 308: return lm_smem_bytes<3, 8>(m);
+    case 316: return lm_smem_bytes<3, 16>(m);
+    default: return lm_smem_bytes<3, 32>(m);
     }
-    const GuessShape shape = guess_shape(m);
-    switch (shape.lanes) {
-    case 8: gs = guess_smem_bytes<8, 16>(m); break;
-    case 16: gs = guess_smem_bytes<16, 16>(m); break;
-    default: gs = shape.v ? guess_smem_bytes<32, 16>(m) : guess_smem_bytes<32, 0>(m); break;
-    }
-    return lm > gs ? lm : gs;
 }
 
-int max_points(int model) {
-    // Largest M whose 32-lane layouts (guess and LM) fit one CTA's 227 KB.
-    const int limit = 227 * 1024;
-    int lo = 1, hi = 1 << 20;
+static int guess_smem(int m) {
+    const GuessShape shape = guess_shape(m);
+    switch (shape.lanes) {
+    case 8: return guess_smem_bytes<8, 16>(m);
+    case 16: return guess_smem_bytes<16, 16>(m);
+    default: return shape.v ? guess_smem_bytes<32, 16>(m) : guess_smem_bytes<32, 0>(m);
+    }
+}
+
+// Largest M with fits(M) (monotone) up to kMaxPoints.
+template <class F> static int largest_m(F fits) {
+    int lo = 1, hi = kMaxPoints;
     while (lo < hi) {
-        const int mid = (lo + hi + 1) / 2;
-        if (smem_bytes(model, 32, mid) <= limit)
+        const int mid = lo + (hi - lo + 1) / 2;
+        if (fits(mid))
             lo = mid;
         else
             hi = mid - 1;
     }
     return lo;
+}
+
+constexpr int kSmemLimit = 227 * 1024;
+
+int group_lm_max_points(int model) {
+    return largest_m([model](int m) { return group_smem_bytes(model, 32, m) <= kSmemLimit; });
+}
+
+int group_guess_max_points() {
+    static const int limit = largest_m([](int m) { return guess_smem(m) <= kSmemLimit; });
+    return limit;
 }
 
 } // namespace bf

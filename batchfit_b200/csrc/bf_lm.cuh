@@ -52,30 +52,47 @@ template <int MODEL> struct Layout {
     __host__ __device__ static constexpr int tri(int k, int l) { return 1 + P + k * (k + 1) / 2 + l; }
 };
 
-// Points a lane accumulates naively before folding chi2 and J^T r into its
-// compensated running sums.
-constexpr int kChunk = 4;
+// Point pairs a lane evaluates between two folds of chi2 and J^T r into its
+// compensated running sums: each half of a pair accumulator sums that many points
+// naively (the even or the odd points of the lane's run).  Measured on B200 (1M
+// pseudo-Voigt fits, M=512; 262,144 two-Lorentzian spectra, M=1024): 4 pairs for the
+// 3- and 4-parameter models, 2 for the two-Lorentzian, whose 8-parameter pass holds
+// more live values per pair.
+template <int MODEL> constexpr int lm_pairs() { return Model<MODEL>::P <= 4 ? 4 : 2; }
 
 // One fused pass at parameters p: state[0] = chi2, state[1..P] = J^T r,
-// state[tri(k,l)] = (J^T J)_kl, as FP64 values.  Returns whether all of them are
-// finite (the reference's linearize() check, solver.hpp:182-190, plus chi2).
+// state[tri(k,l)] = (J^T J)_kl, as FP64 values.
 //
-// Accumulation: each lane sums kChunk points naively, then folds the chunk's chi2
-// and J^T r into Kahan pairs (numerics::add, numerics.hpp:12-18); the pairs enter
-// a two-sum reduce-scatter across the group with their low parts.  J^T r decides
-// where the iteration stops (its error moves the fixed point), so it gets the
-// compensation; J^T J only shapes the step and takes a plain reduce-scatter.
-template <int MODEL, int G>
-__device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, const float *ys, int m,
-                                        const float *p, double *state) {
-    using L = Layout<MODEL>;
-    constexpr int P = L::P;
-    constexpr int KC = P + 1;                 // chi2 and J^T r
-    constexpr int KCP = reduce_slots(KC, G);
-    constexpr int T = P * (P + 1) / 2;        // J^T J lower triangle
-    constexpr int TP = reduce_slots(T, G);
-    const auto q = Model<MODEL>::prepare(p);
-    float hi[KCP], lo[KCP], aa[TP];
+// Evaluation: each lane takes two adjacent points at a time and evaluates them with
+// packed float32 pairs (sm_100 f32x2: one instruction, two IEEE results), so the
+// model, the residual and every accumulation cost half the issue slots of scalar
+// code.  Lane `lane` of LANES takes the pairs starting at 2 lane, 2 (lane + LANES),
+// ...  PAIRED_LOADS: xs and ys are 8-byte aligned (shared-memory copies, or aligned
+// global rows) and a pair is read with one load; otherwise point by point.  Both
+// give identical results.
+//
+// Accumulation: the pair accumulators of a lane sum a few pairs naively; the two
+// halves are then added and folded into Kahan pairs for chi2 and J^T r
+// (numerics::add, numerics.hpp:12-18), which enter a two-sum reduce-scatter with
+// their low parts.  J^T r decides where the iteration stops (its error moves the
+// fixed point), so it gets the compensation; J^T J only shapes the step and takes
+// a plain reduce-scatter.  For P <= 4, J^T J is summed in pairs too (2 T
+// registers); the 8-parameter model keeps scalar sums of its 36 J^T J terms, which
+// would not fit the registers twice.
+//
+// pass_sums leaves a lane's partial sums in hi/lo (chi2, J^T r; value hi + lo) and
+// aa (J^T J lower triangle); slots past KC and T are zero.
+template <int MODEL, int LANES, bool PAIRED_LOADS, int KCP, int TP>
+__device__ __forceinline__ void pass_sums(int lane, const float *xs, const float *ys, int m, const float *p,
+                                          float (&hi)[KCP], float (&lo)[KCP], float (&aa)[TP]) {
+    constexpr int P = Model<MODEL>::P;
+    constexpr int KC = P + 1;          // chi2 and J^T r
+    constexpr int T = P * (P + 1) / 2; // J^T J lower triangle
+    constexpr bool kPairedA = P <= 4;
+    constexpr int kPairs = lm_pairs<MODEL>();
+    static_assert(KCP >= KC && TP >= T, "slot arrays");
+    const auto q = Model<MODEL>::prepare2(p);
+    float2 aa2[kPairedA ? T : 1];
 #pragma unroll
     for (int i = 0; i < KCP; ++i) {
         hi[i] = 0.0f;
@@ -84,53 +101,111 @@ __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, cons
 #pragma unroll
     for (int i = 0; i < TP; ++i)
         aa[i] = 0.0f;
-    // Full chunks without per-point bounds checks, then one masked tail chunk.
-    const int full = m - m % (G * kChunk);
-    auto point = [&](int j, float (&part)[KC]) {
-        float J[P];
-        const float r = Model<MODEL>::residual(q, xs[j], ys[j], J);
-        part[0] = fmaf(r, r, part[0]);
 #pragma unroll
-        for (int k = 0; k < P; ++k) {
-            part[1 + k] = fmaf(J[k], r, part[1 + k]);
-#pragma unroll
-            for (int l = 0; l <= k; ++l)
-                aa[k * (k + 1) / 2 + l] = fmaf(J[k], J[l], aa[k * (k + 1) / 2 + l]);
+    for (int i = 0; i < (kPairedA ? T : 1); ++i)
+        aa2[i] = splat2(0.0f);
+    // Points j and j + 1 (j even); `second` false: j + 1 is past the end -- it is not
+    // read, and the pair's second half adds nothing.  xs and ys may be shared or
+    // global memory: generic loads only.
+    auto load = [&](int j, bool second, float2 &xv, float2 &yv) {
+        if (PAIRED_LOADS && second) {
+            xv = *reinterpret_cast<const float2 *>(xs + j);
+            yv = *reinterpret_cast<const float2 *>(ys + j);
+        } else {
+            xv.x = xs[j];
+            yv.x = ys[j];
+            xv.y = second ? xs[j + 1] : xv.x;
+            yv.y = second ? ys[j + 1] : yv.x;
         }
     };
-    // Kahan fold; lo holds minus the Kahan correction, so the value is hi + lo.
-    auto fold = [&](const float (&part)[KC]) {
+    auto pair = [&](float2 xv, float2 yv, bool second, float2 (&part)[KC]) {
+        float2 J[P];
+        float2 r = Model<MODEL>::residual2(q, xv, yv, J);
+        if (!second) {
+            r.y = 0.0f;
+#pragma unroll
+            for (int k = 0; k < P; ++k)
+                J[k].y = 0.0f;
+        }
+        part[0] = fma2(r, r, part[0]);
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            part[1 + k] = fma2(J[k], r, part[1 + k]);
+#pragma unroll
+            for (int l = 0; l <= k; ++l) {
+                const int t = k * (k + 1) / 2 + l;
+                if constexpr (kPairedA) {
+                    aa2[t] = fma2(J[k], J[l], aa2[t]);
+                } else {
+                    aa[t] = fmaf(J[k].x, J[l].x, aa[t]);
+                    aa[t] = fmaf(J[k].y, J[l].y, aa[t]);
+                }
+            }
+        }
+    };
+    // Kahan fold of both halves; lo holds minus the Kahan correction, so the value is hi + lo.
+    auto fold = [&](const float2 (&part)[KC]) {
 #pragma unroll
         for (int i = 0; i < KC; ++i) {
-            const float adjusted = __fadd_rn(part[i], lo[i]);
+            const float adjusted = __fadd_rn(__fadd_rn(part[i].x, part[i].y), lo[i]);
             const float next = __fadd_rn(hi[i], adjusted);
             lo[i] = __fsub_rn(adjusted, __fsub_rn(next, hi[i]));
             hi[i] = next;
         }
     };
-    for (int base = int(g.lane); base < full; base += G * kChunk) {
-        float part[KC];
+    // Full runs of kPairs pairs per lane without bounds checks, then one masked tail.
+    constexpr int span = 2 * LANES * kPairs;
+    const int full = m - m % span;
+    for (int base = 2 * lane; base < full; base += span) {
+        float2 part[KC];
 #pragma unroll
         for (int i = 0; i < KC; ++i)
-            part[i] = 0.0f;
+            part[i] = splat2(0.0f);
 #pragma unroll
-        for (int c = 0; c < kChunk; ++c)
-            point(base + c * G, part);
-        fold(part);
-    }
-    if (full < m) {
-        float part[KC];
-#pragma unroll
-        for (int i = 0; i < KC; ++i)
-            part[i] = 0.0f;
-#pragma unroll
-        for (int c = 0; c < kChunk; ++c) {
-            const int j = full + int(g.lane) + c * G;
-            if (j < m)
-                point(j, part);
+        for (int c = 0; c < kPairs; ++c) {
+            float2 xv, yv;
+            load(base + 2 * LANES * c, true, xv, yv);
+            pair(xv, yv, true, part);
         }
         fold(part);
     }
+    if (full < m) {
+        float2 part[KC];
+#pragma unroll
+        for (int i = 0; i < KC; ++i)
+            part[i] = splat2(0.0f);
+#pragma unroll
+        for (int c = 0; c < kPairs; ++c) {
+            const int j = full + 2 * lane + 2 * LANES * c;
+            if (j < m) {
+                const bool second = j + 1 < m;
+                float2 xv, yv;
+                load(j, second, xv, yv);
+                pair(xv, yv, second, part);
+            }
+        }
+        fold(part);
+    }
+    if constexpr (kPairedA) {
+#pragma unroll
+        for (int t = 0; t < T; ++t)
+            aa[t] = __fadd_rn(aa2[t].x, aa2[t].y);
+    }
+}
+
+// The pass of one group: the group's lanes reduce their sums into `state`.
+// Returns whether every sum is finite (the reference's linearize() check,
+// solver.hpp:182-190, plus chi2).
+template <int MODEL, int G, bool PAIRED_LOADS>
+__device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, const float *ys, int m,
+                                        const float *p, double *state) {
+    constexpr int P = Model<MODEL>::P;
+    constexpr int KC = P + 1;
+    constexpr int KCP = reduce_slots(KC, G);
+    constexpr int T = P * (P + 1) / 2;
+    constexpr int TP = reduce_slots(T, G);
+    float hi[KCP], lo[KCP], aa[TP];
+    pass_sums<MODEL, G, PAIRED_LOADS>(int(g.lane), xs, ys, m, p, hi, lo, aa);
     bool finite = reduce_scatter_store<G, KCP>(g, hi, lo, state, KC);
     finite = reduce_scatter_store_plain<G, TP>(g, aa, state + KC, T) && finite;
     finite = g.all(finite);
@@ -261,8 +336,8 @@ template <int MODEL> __device__ __forceinline__ void lm_begin(const FitArgs &a, 
 
 // Consume the pass that just wrote slot 1 - s.cur.  Returns true when the fit is
 // finished (s.status final).
-template <int MODEL, int G>
-__device__ __forceinline__ bool lm_after_pass(const Group<G> &g, const FitArgs &a, const XConst &xc, bool y_flat,
+template <int MODEL, class Grp>
+__device__ __forceinline__ bool lm_after_pass(const Grp &g, const FitArgs &a, const XConst &xc, bool y_flat,
                                               bool pass_finite, const double *state, LmState<MODEL> &s) {
     using L = Layout<MODEL>;
     const double c = state[(1 - s.cur) * L::K];
@@ -557,8 +632,8 @@ __device__ int covariance_one(const FitArgs &a, const float *p, int fit_status, 
 }
 
 // Outputs of a finished fit (FitResult, solver.hpp:43-48).
-template <int MODEL, int G>
-__device__ __forceinline__ void write_fit(const Group<G> &g, const FitArgs &a, long long fit, const LmState<MODEL> &s) {
+template <int MODEL, class Grp>
+__device__ __forceinline__ void write_fit(const Grp &g, const FitArgs &a, long long fit, const LmState<MODEL> &s) {
     constexpr int P = Model<MODEL>::P;
 #pragma unroll
     for (int k = 0; k < P; ++k)
@@ -573,11 +648,11 @@ __device__ __forceinline__ void write_fit(const Group<G> &g, const FitArgs &a, l
 
 // The accepted J^T J (the information matrix at the reported parameters), left in
 // the covariance output for the covariance kernel.
-template <int MODEL, int G>
-__device__ __forceinline__ void write_information(const Group<G> &g, const FitArgs &a, long long fit,
+template <int MODEL, class Grp>
+__device__ __forceinline__ void write_information(const Grp &g, const FitArgs &a, long long fit,
                                                   const double *cur) {
     constexpr int P = Model<MODEL>::P;
-    for (int k = int(g.lane); k < P * P; k += G) {
+    for (int k = int(g.lane); k < P * P; k += Grp::size) {
         const int i = k / P, j = k % P;
         a.covariance[fit * P * P + k] = float(cur[Layout<MODEL>::tri(i > j ? i : j, i > j ? j : i)]);
     }

@@ -75,6 +75,12 @@ int bf_cuda_fit_noalloc(const bf_fit_args *args, const bf_fit_outputs *out, void
             "bf_cuda_fit_noalloc: N=" + std::to_string(args->n) + " fits without p0 exceed the " +
                 std::to_string(max_guessed_fits(args->model)) +
                 " whose guesses fit the 4 MiB no-allocation scratch; pass p0 or split the batch");
+    if (!args->p0 && args->m > uint32_t(bf::long_guess_smem_max_points()))
+        return bf::host::report(
+            BF_ERR_INVALID_ARGUMENT,
+            "bf_cuda_fit_noalloc: data-only guesses of M=" + std::to_string(args->m) +
+                " points need scratch beyond shared memory (M up to " +
+                std::to_string(bf::long_guess_smem_max_points()) + " without p0); pass p0");
     unsigned char *scratch = nullptr;
     rc = scratch_in_current_context(&scratch);
     if (rc != BF_OK)

@@ -56,9 +56,20 @@ struct Request {
     bf_batch_segment seg{};     // the request with device pointers
     Clock::time_point submitted, done;
     int result = BF_OK;
-    bool charged = false; // its bytes count against the budget (admitted)
+    bool charged = false;   // its bytes count against the budget (admitted)
+    bool cancelled = false; // cancelled before admission: completes with BF_ERR_CANCELLED
     bool finished = false;
 };
+
+// Predicted device time of a request (ms): N * M points at the per-point cost of
+// its model's kernels (guess + LM), measured on B200 at the benchmark sizes.  Only
+// ratios matter: the scheduler uses it to keep batches short.
+double predicted_ms(const bf_fit_args &a) {
+    static constexpr double kNsPerPoint[4] = {0.010, 0.010, 0.014, 0.10};
+    return double(a.n) * double(a.m) * kNsPerPoint[a.model & 3] * 1e-6;
+}
+// A batch grows to about this much predicted device time; a larger request runs alone.
+constexpr double kBatchTargetMs = 1.0;
 
 // Device bytes of a request: x, y, p0, outputs, plus the batch arena's per-fit
 // share (work items and guesses).
@@ -97,6 +108,7 @@ struct bf_server {
     std::map<uint64_t, std::shared_ptr<Request>> tickets; // every unreleased request
     bf_server_stats stats{};
     std::string fatal; // a CUDA failure that stopped the scheduler
+    uint32_t fail_allocations = 0; // host-side fault injection (bf_server_fail_allocations)
 
     // Scheduler-owned state.
     std::deque<std::shared_ptr<Request>> pending;  // waiting for admission
@@ -127,19 +139,41 @@ void complete(bf_server *s, const std::shared_ptr<Request> &r, int result) {
 bool admit(bf_server *s) {
     std::shared_ptr<CopyMark> mark;
     while (!s->pending.empty()) {
-        const std::shared_ptr<Request> &r = s->pending.front();
+        const std::shared_ptr<Request> r = s->pending.front();
+        bool cancelled = false, inject = false;
         {
             std::lock_guard<std::mutex> lock(s->mutex);
-            if (s->stats.memory_in_use + r->bytes > s->stats.memory_budget)
-                break;
-            s->stats.memory_in_use += r->bytes;
-            s->stats.memory_peak = std::max(s->stats.memory_peak, s->stats.memory_in_use);
-            r->charged = true;
+            cancelled = r->cancelled;
+            if (!cancelled) {
+                if (s->stats.memory_in_use + r->bytes > s->stats.memory_budget)
+                    break;
+                s->stats.memory_in_use += r->bytes;
+                s->stats.memory_peak = std::max(s->stats.memory_peak, s->stats.memory_in_use);
+                r->charged = true;
+                if (s->fail_allocations) {
+                    s->fail_allocations -= 1;
+                    inject = true;
+                }
+            }
+        }
+        if (cancelled) {
+            s->pending.pop_front();
+            complete(s, r, BF_ERR_CANCELLED);
+            continue;
         }
         const bf_fit_args &a = r->args;
         const size_t n = a.n, m = a.m, p = size_t(parameters(a.model));
         void *block = nullptr;
-        cudaError_t e = cudaMallocFromPoolAsync(&block, r->bytes, s->pool, s->copy);
+        cudaError_t e = inject ? cudaErrorMemoryAllocation : cudaMallocFromPoolAsync(&block, r->bytes, s->pool, s->copy);
+        if (e == cudaErrorMemoryAllocation) {
+            // The request fails alone: its bytes return to the budget and the
+            // server goes on with the others.
+            if (!inject)
+                cudaGetLastError();
+            s->pending.pop_front();
+            complete(s, r, BF_ERR_CUDA);
+            continue;
+        }
         if (e != cudaSuccess) {
             report_cuda(e, "server allocation");
             return false;
@@ -204,26 +238,47 @@ bool launch(bf_server *s, Slot &slot) {
     // Copies complete in admission order, so the requests whose inputs are on the
     // device are a prefix of the ready list: a batch never waits for other
     // requests' copies.
+    //
+    // Batches are kept short so that a small request never waits for a large one:
+    // requests join in arrival order while the batch's predicted device time stays
+    // within kBatchTargetMs; a request predicted to take longer runs alone (it starts
+    // a batch, or waits for the next free slot), and later small requests may pass it.
     std::vector<std::shared_ptr<Request>> take;
+    std::vector<bool> taken(s->ready.size(), false);
     uint64_t fits = 0;
-    size_t i = 0;
-    for (; i < s->ready.size(); ++i) {
-        const uint64_t n = s->ready[i]->args.n;
-        if (!take.empty() && s->opt.max_batch_fits && fits + n > s->opt.max_batch_fits)
-            break;
-        const cudaError_t q = cudaEventQuery(s->ready[i]->copied->event);
+    double predicted = 0.0;
+    for (size_t i = 0; i < s->ready.size(); ++i) {
+        const std::shared_ptr<Request> &r = s->ready[i];
+        const uint64_t n = r->args.n;
+        const double t = predicted_ms(r->args);
+        const cudaError_t q = cudaEventQuery(r->copied->event);
         if (q == cudaErrorNotReady)
             break;
         if (q != cudaSuccess) {
             report_cuda(q, "server copy-in");
             return false;
         }
-        take.push_back(s->ready[i]);
+        if (!take.empty() && s->opt.max_batch_fits && fits + n > s->opt.max_batch_fits)
+            break;
+        if (!take.empty() && predicted + t > kBatchTargetMs) {
+            if (t > kBatchTargetMs)
+                continue; // large: its own batch, later
+            break;
+        }
+        take.push_back(r);
+        taken[i] = true;
         fits += n;
+        predicted += t;
+        if (predicted > kBatchTargetMs)
+            break; // a large request alone
     }
     if (take.empty())
         return true;
-    s->ready.erase(s->ready.begin(), s->ready.begin() + i);
+    size_t keep = 0;
+    for (size_t i = 0; i < s->ready.size(); ++i)
+        if (!taken[i])
+            s->ready[keep++] = s->ready[i];
+    s->ready.resize(keep);
     std::vector<bf_batch_segment> segs;
     segs.reserve(take.size());
     for (auto &r : take)
@@ -544,6 +599,29 @@ int bf_server_wait(bf_server *s, uint64_t ticket, double *latency_ms) {
         *latency_ms = std::chrono::duration<double, std::milli>(r->done - r->submitted).count();
     if (r->result != BF_OK)
         return report(r->result, s->fatal.empty() ? "request failed" : "request failed: " + s->fatal);
+    return BF_OK;
+}
+
+int bf_server_cancel(bf_server *s, uint64_t ticket) {
+    if (!s)
+        return -BF_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(s->mutex);
+    auto it = s->tickets.find(ticket);
+    if (it == s->tickets.end())
+        return -BF_ERR_INVALID_ARGUMENT;
+    Request &r = *it->second;
+    if (r.finished || r.charged || r.cancelled)
+        return r.cancelled ? 1 : 0;
+    r.cancelled = true; // the scheduler completes it before admission
+    s->wake.notify_one();
+    return 1;
+}
+
+int bf_server_fail_allocations(bf_server *s, uint32_t count) {
+    if (!s)
+        return report(BF_ERR_INVALID_ARGUMENT, "null server");
+    std::lock_guard<std::mutex> lock(s->mutex);
+    s->fail_allocations = count;
     return BF_OK;
 }
 

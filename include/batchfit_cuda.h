@@ -42,6 +42,7 @@ extern "C" {
 #define BF_ERR_CUDA 2             /* a CUDA runtime error (std::runtime_error) */
 #define BF_ERR_UNAVAILABLE 3      /* no usable sm_100 device */
 #define BF_ERR_BUSY 4             /* a pending submission still owns the context */
+#define BF_ERR_CANCELLED 5        /* a server request cancelled before it was admitted */
 
 /* Model ids (python/batchfit/__init__.py:13). */
 #define BF_MODEL_GAUSSIAN 0       /* amplitude, center, sigma */
@@ -96,7 +97,7 @@ typedef struct bf_fit_args {
     const float *p0;   /* [N*P] initial values, or NULL for data-only guesses */
     int32_t memory;    /* BF_MEMORY_* for x, y, p0 and every output */
     int32_t uncertainties;
-    int32_t group_lanes; /* 0 = tuned choice, else 8, 16 or 32 lanes per fit */
+    int32_t group_lanes; /* 0 = tuned choice, else 8, 16 or 32 lanes per fit, or 128 = one CTA per fit */
     bf_solver_options options;
     int32_t y_format;    /* BF_Y_FLOAT32, or BF_Y_FLOAT16 (bf_cuda_fit / submit only) */
 } bf_fit_args;
@@ -162,7 +163,9 @@ int bf_cuda_last_timing(bf_cuda_context *ctx, bf_cuda_timing *out);
 int bf_cuda_host_alloc(size_t bytes, void **out);
 int bf_cuda_host_free(void *ptr);
 
-/* Largest M the kernels support for `model` (shared-memory layout bound). */
+/* Largest M bf_cuda_fit takes for `model`.  Spectra that do not fit the group
+ * kernels' shared-memory layouts run one CTA (128 threads) per fit, reading x and y
+ * through L2, with a long-spectrum guess; they take float32 y. */
 uint32_t bf_cuda_max_points(int32_t model);
 
 /* ---- Mixed batches --------------------------------------------------------
@@ -216,7 +219,9 @@ int bf_cuda_set_tuning(bf_cuda_context *ctx, const bf_tuning *in);
  * coalesced into mixed batches (bf_cuda_fit_batch's kernels).  Up to two batches
  * are on the GPU at once, on two streams: requests that arrive while a batch runs
  * form the next one, which starts as soon as they are copied in and overlaps the
- * running batch's tail.  Outputs are copied into the request's host buffers, which
+ * running batch's tail.  A batch grows to about 1 ms of predicted device time; a
+ * request predicted to take longer runs in a batch of its own, and smaller requests
+ * that arrive after it may start before it.  Outputs are copied into the request's host buffers, which
  * stay owned by the caller and must stay valid until the request completes.  A
  * request's result is the one bf_cuda_fit_batch gives for it; batch-mates only
  * change its lanes per fit (so results agree within the parity tolerances). */
@@ -248,6 +253,16 @@ int bf_server_poll(bf_server *server, uint64_t ticket);
  * *latency_ms (optional) = submit to outputs written. */
 int bf_server_wait(bf_server *server, uint64_t ticket, double *latency_ms);
 int bf_server_get_stats(bf_server *server, bf_server_stats *out);
+/* Cancels a request that has not been admitted yet: returns 1 when it is cancelled
+ * (its wait returns BF_ERR_CANCELLED), 0 when it is already admitted or finished
+ * (it completes normally), -BF_ERR_INVALID_ARGUMENT for an unknown ticket. */
+int bf_server_cancel(bf_server *server, uint64_t ticket);
+/* Failure injection for tests of the failure handling, on the host: the next
+ * `count` admissions fail as if the device allocation had run out of memory.  Such
+ * a request completes with BF_ERR_CUDA, its bytes return to the budget and the
+ * server carries on with the other requests (a real out-of-memory allocation is
+ * handled the same way). */
+int bf_server_fail_allocations(bf_server *server, uint32_t count);
 
 /* ---- NPY streaming -----------------------------------------------------------
  * Out-of-core fits straight from .npy files: the reference's metal::fit_npy

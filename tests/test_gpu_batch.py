@@ -172,11 +172,14 @@ def test_mixed_uneven_stream_matches_oracle(bf, oracle):
     # definite status: on this workload they are unresolved peaks (FWHM below the
     # grid spacing) that the reference's own float32 path reports as unresolved.
     # They must not converge on the GPU either.  On every other fit statuses agree
-    # at the parity bar, and the GPU's parameters are at least as often within 1e-4
-    # of the float64 solution as the reference's own float32 solver's are (the
-    # stream holds unresolved and overlapping peaks whose parameters no float32
-    # solver pins to 1e-4).
-    definite = agree = within = within_ref32 = chi2_ok = converged = 0
+    # at the parity bar (>= 99.9%); the single-peak models are within 1e-4 / 1e-5
+    # of the float64 solution for >= 99% of their converged fits; and >= 99.5% of all
+    # converged fits are within or float32-equivalent (float64 chi2 within the
+    # float32 evaluation error of the oracle's): the two-Lorentzian requests hold
+    # overlapping doublets whose parameters no float32 evaluation pins to 1e-4.
+    definite = agree = chi2_ok = converged = 0
+    within = {m: [0, 0] for m in names}
+    equivalent = within_ref32 = within_all = 0
     for r, g in zip(reqs, got):
         lo, hi = r["bounds"]
         ref = oracle.fit("port", r["model"], r["x"], r["y"], None, lo, hi, np.float64)
@@ -186,19 +189,26 @@ def test_mixed_uneven_stream_matches_oracle(bf, oracle):
             continue
         ref32 = oracle.fit("port", r["model"], r["x"], r["y"], None, lo, hi, np.float32)
         s = A.summarize(r["model"], r["x"], r["y"], g.params.cpu().numpy(), gs, g.chi2.cpu().numpy(), ref.params,
-                        ref.status, ref.chi2, PARAM_TOL, CHI2_TOL)
+                        ref.status, ref.chi2, PARAM_TOL, CHI2_TOL, x64=True)
         s32 = A.summarize(r["model"], r["x"], r["y"], ref32.params, ref32.status, ref32.chi2, ref.params,
                           ref.status, ref.chi2, PARAM_TOL, CHI2_TOL)
         definite += 1
         agree += s["status_agreement"]
-        within += s["within_tol_fraction"]
+        within_all += s["within_tol_fraction"]
         within_ref32 += s32["within_tol_fraction"]
+        if ref.status[0] in (0, 5) and gs[0] == ref.status[0]:
+            within[r["model"]][0] += s["within_tol_fraction"]
+            within[r["model"]][1] += 1
+            equivalent += s["within_or_equivalent_fraction"]
         if ref.status[0] == 0 and gs[0] == 0:
             converged += 1
             chi2_ok += s["chi2_within_fraction"]
     assert definite >= 1150
     assert agree / definite >= STATUS_AGREE, (agree, definite)
-    assert within >= within_ref32, (within, within_ref32, definite)
+    for model in ("gaussian", "lorentzian", "pseudo_voigt"):
+        assert within[model][0] >= 0.99 * within[model][1], (model, within[model])
+    assert equivalent >= 0.995 * sum(v[1] for v in within.values()), (equivalent, within)
+    assert within_all >= within_ref32, (within_all, within_ref32, definite)
     assert chi2_ok / converged >= STATUS_AGREE, (chi2_ok, converged)
 
 

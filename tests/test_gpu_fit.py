@@ -315,42 +315,96 @@ def test_async_submit_wait(bf):
 
 def test_two_lorentzian_cube_sample_parity(bf, oracle):
     """The overlapping-peak cube (M=1024, 5% pure-noise and 2% constant rows) on a
-    3,000-row sample, against the float64 oracle where it reaches a definite
-    status: statuses agree and parameters are within 1e-4 at least as often as the
-    reference's own float32 solver's do (this stress case is ill-conditioned: the
-    float32 reference agrees on 99.1% of statuses and 74% of parameters); rows
-    without two resolvable peaks get no guess (invalid input, as the reference)."""
+    3,000-row sample against the float64 oracle.
+
+    Statuses agree on >= 99.5% of the fits the oracle ends with a definite status
+    (not max_iterations).  Converged fits are within 1e-4 / 1e-5 of the oracle or
+    float32-equivalent to it (their float64 chi2 is within the float32 evaluation
+    error of the oracle's) for >= 96% -- and more often than the reference's own
+    float32 solver's.  Plain 1e-4 agreement is out of reach on this stress case for
+    any float32 evaluation: ~40% of its converged fits lie in valleys flatter than
+    float32 chi2 can resolve (the float64 oracle itself moves by more than 1e-4 on
+    ~4% of them when its own tolerances are tightened).  Rows without two
+    resolvable peaks get no guess (invalid input, as the reference)."""
     w = W.two_lorentzian_cube(n=3000, seed=3)
     got = bf.fit(w.x, w.y, w.model, None, (w.lower, w.upper), "cuda")
     ref = oracle.fit("port", w.model, w.x, w.y, None, w.lower, w.upper, np.float64)
     ref32 = oracle.fit("port", w.model, w.x, w.y, None, w.lower, w.upper, np.float32)
-    definite = ref.status != 1
-    s = A.summarize(w.model, w.x, w.y[definite], got.params[definite], got.status[definite], got.chi2[definite],
-                    ref.params[definite], ref.status[definite], ref.chi2[definite], PARAM_TOL, CHI2_TOL)
-    s32 = A.summarize(w.model, w.x, w.y[definite], ref32.params[definite], ref32.status[definite],
-                      ref32.chi2[definite], ref.params[definite], ref.status[definite], ref.chi2[definite],
-                      PARAM_TOL, CHI2_TOL)
-    assert definite.mean() >= 0.95
-    assert s["status_agreement"] >= s32["status_agreement"], (s, s32)
+    s = A.summarize(w.model, w.x, w.y, got.params, got.status, got.chi2, ref.params, ref.status, ref.chi2,
+                    PARAM_TOL, CHI2_TOL, x64=True)
+    s32 = A.summarize(w.model, w.x, w.y, ref32.params, ref32.status, ref32.chi2, ref.params, ref.status, ref.chi2,
+                      PARAM_TOL, CHI2_TOL, x64=True)
+    assert s["definite_fraction"] >= 0.95
+    assert s["status_agreement_definite"] >= 0.995, s
+    assert s["status_agreement_definite"] >= s32["status_agreement_definite"], (s, s32)
+    assert s["within_or_equivalent_fraction"] >= 0.96, s
+    assert s["within_or_equivalent_fraction"] >= s32["within_or_equivalent_fraction"], (s, s32)
     assert s["within_tol_fraction"] >= s32["within_tol_fraction"], (s, s32)
     assert np.all(got.status[w.meta["constant"]] == 3)
     np.testing.assert_array_equal(got.status[w.meta["noise_only"]], ref.status[w.meta["noise_only"]])
 
 
+@pytest.mark.parametrize("m", [4096, 8192, 32768])
 @pytest.mark.parametrize("model", ["gaussian", "lorentzian", "pseudo_voigt", "two_lorentzian"])
-def test_largest_supported_m(bf, oracle, model):
-    """The largest M the shared-memory kernels take (groups widen to whole warps):
-    parity with the float64 oracle holds there, and one point more is refused."""
-    m = int(bf._capi.load().bf_cuda_max_points(bf.MODELS[model]))
-    x, y, lo, hi = synthetic(model, 24, m, seed=11 + m)
-    got = bf.fit(x, y, model, None, (lo, hi), "cuda")
-    ref = oracle.fit("port", model, x, y, None, lo, hi, np.float64)
+def test_long_spectra_match_the_oracle(bf, oracle, model, m):
+    """Any M the reference fits: spectra beyond the group kernels' shared-memory
+    layouts run one CTA per fit (and the long-spectrum guess); parity with the
+    float64 oracle holds there, with uncertainties, and the guesses equal the
+    reference's float guesses bit for bit."""
+    n = 24 if m <= 8192 else 8
+    x, y, lo, hi = synthetic(model, n, m, seed=11 + m)
+    got = bf.fit(x, y, model, None, (lo, hi), "cuda", uncertainties=True)
+    ref = oracle.fit("port", model, x, y, None, lo, hi, np.float64, uncertainties=True)
     s = A.summarize(model, x, y, got.params, got.status, got.chi2, ref.params, ref.status, ref.chi2, PARAM_TOL,
                     CHI2_TOL)
-    assert s["status_agreement"] >= 23 / 24 and s["within_tol_fraction"] >= 22 / 24, s
+    assert s["status_agreement"] == 1.0 and s["within_tol_fraction"] >= (n - 1) / n, s
+    gp, gs = bf.guess(x, y, model)
+    rp, rs, _ = oracle.guess("port", model, x, y, np.float32)
+    np.testing.assert_array_equal(gs, rs)
+    np.testing.assert_array_equal(gp, rp)
+    np.testing.assert_array_equal(got.uncertainty_status, ref.uncertainty_status)
+    ok = got.uncertainty_status == 0
+    np.testing.assert_allclose(got.stderr[ok], ref.stderr[ok], rtol=5e-3)
+
+
+@pytest.mark.parametrize("model", ["lorentzian", "two_lorentzian"])
+def test_cta_per_fit_mapping_on_group_sized_spectra(bf, oracle, model):
+    """group_lanes=128 forces the CTA-per-fit kernel where the group kernels would
+    run; both mappings agree with the float64 oracle on the same spectra, with
+    ragged M (odd, not a multiple of the pair span)."""
+    x, y, lo, hi = synthetic(model, 64, 777, seed=5)
+    ref = oracle.fit("port", model, x, y, None, lo, hi, np.float64)
+    for lanes in (0, 128):
+        got = bf.fit(x, y, model, None, (lo, hi), "cuda", group_lanes=lanes)
+        s = A.summarize(model, x, y, got.params, got.status, got.chi2, ref.params, ref.status, ref.chi2, PARAM_TOL,
+                        CHI2_TOL)
+        assert s["status_agreement"] == 1.0 and s["within_tol_fraction"] >= 63 / 64, (lanes, s)
+
+
+def test_long_spectrum_guess_beyond_shared_memory(bf, oracle):
+    """M large enough that the long-spectrum guess keeps its sort scratch in global
+    memory: guesses still equal the reference's float guess bit for bit, and the
+    fits the float64 oracle."""
+    m = 200_000
+    x, y, lo, hi = synthetic("lorentzian", 3, m, seed=3)
+    gp, gs = bf.guess(x, y, "lorentzian")
+    rp, rs, _ = oracle.guess("port", "lorentzian", x, y, np.float32)
+    np.testing.assert_array_equal(gs, rs)
+    np.testing.assert_array_equal(gp, rp)
+    got = bf.fit(x, y, "lorentzian", None, (lo, hi), "cuda")
+    ref = oracle.fit("port", "lorentzian", x, y, None, lo, hi, np.float64)
+    s = A.summarize("lorentzian", x, y, got.params, got.status, got.chi2, ref.params, ref.status, ref.chi2,
+                    PARAM_TOL, CHI2_TOL)
+    assert s["status_agreement"] == 1.0 and s["within_tol_fraction"] == 1.0, s
+
+
+def test_beyond_the_largest_m_is_refused(bf):
+    m = int(bf._capi.load().bf_cuda_max_points(bf.MODELS["lorentzian"]))
+    assert m >= 1 << 20
+    lo, hi = np.array([0, -10, 1e-3], np.float32), np.array([np.inf, 10, 10], np.float32)
     x2 = np.linspace(-10, 10, m + 1).astype(np.float32)
     with pytest.raises(ValueError, match="exceeds"):
-        bf.fit(x2, np.zeros((1, m + 1), np.float32), model, None, (lo, hi), "cuda")
+        bf.fit(x2, np.zeros((1, m + 1), np.float32), "lorentzian", None, (lo, hi), "cuda")
 
 
 @pytest.mark.parametrize("m", [1, 2, 4, 5, 6])
@@ -390,3 +444,7 @@ def test_half_precision_y_equals_float_of_the_same_values(bf):
         np.testing.assert_array_equal(dev.params.cpu().numpy(), full.params)
     with pytest.raises(TypeError):
         bf.fit_batch([dict(x=torch.as_tensor(x).cuda(), y=torch.as_tensor(y16).cuda(), model="pseudo_voigt")])
+    # Long spectra (one CTA per fit) read y straight from global memory: float32 only.
+    xl, yl, lo, hi = synthetic("pseudo_voigt", 2, 16384, seed=1)
+    with pytest.raises(ValueError, match="float32"):
+        bf.fit(xl, yl.astype(np.float16), "pseudo_voigt", None, (lo, hi), "cuda")

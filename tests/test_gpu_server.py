@@ -131,3 +131,43 @@ def test_close_completes_outstanding_requests(bf):
         alone = bf.fit_batch([dict(r, uncertainties=False)])[0]
         a, w, n = same_within_tolerance(r, got, alone)
         assert a >= 0.99
+
+
+def test_allocation_failure_and_cancellation_leave_the_others_intact(bf):
+    """Failure handling on the host, without a GPU fault: an admission whose device
+    allocation fails (injected: the next admission's allocation reports out of
+    memory) fails alone with a CUDA error, a request cancelled before admission
+    raises CancelledError, and every other request completes with the result it
+    gives alone; the memory budget returns to zero and the server keeps serving."""
+    import concurrent.futures
+
+    reqs = make_requests(9, seed=21, n_max=300, m_range=(1024, 1024))
+    last = make_requests(1, seed=22, n_max=2, m_range=(1024, 1024))[0]
+    last["y"] = np.repeat(last["y"][:1], 300, axis=0)
+    reqs.append(last)
+    # A budget of about one request (300 x 1024 points take ~1.3 MB) admits them
+    # nearly one at a time, strictly in arrival order: the last one stays queued
+    # behind the others while it is cancelled.
+    budget = 2 << 20
+    with bf.Server(memory_budget=budget, max_in_flight=1) as server:
+        server._fail_allocations(1)
+        tickets = [server.submit(r["x"], r["y"], r["model"], None, r["bounds"], uncertainties=r["uncertainties"])
+                   for r in reqs]
+        assert tickets[-1].cancel()
+        assert tickets[-1].cancel()  # idempotent
+        with pytest.raises(RuntimeError, match="failed"):
+            tickets[0].result()  # the first admission took the injected failure
+        with pytest.raises(concurrent.futures.CancelledError):
+            tickets[-1].result()
+        results = [t.result() for t in tickets[1:-1]]
+        assert not tickets[1].cancel()  # completed requests cannot be cancelled
+        st = server.stats()
+        assert st["memory_in_use"] == 0
+        assert st["failed"] == 2 and st["completed"] == len(reqs)
+        # Still serving after the failures.
+        again = server.submit(reqs[0]["x"], reqs[0]["y"], reqs[0]["model"], None, reqs[0]["bounds"]).result()
+        assert again.status.shape == (reqs[0]["y"].shape[0],)
+    for r, got in zip(reqs[1:-1], results):
+        alone = bf.fit_batch([r])[0]
+        a, w, n = same_within_tolerance(r, got, alone)
+        assert a >= 0.99 and w >= 0.99
