@@ -410,7 +410,10 @@ __device__ __forceinline__ bool lm_plan(const FitArgs &a, const XConst &xc, doub
         bool active[P];
         double gnorm = 0.0;
         bool at_floor = true;
-        const double floor_g = a.noise_floor * kFltEps * sqrt(syy);
+        // |g_k| <= floor * eps * sqrt(A_kk * sum(y^2)), compared squared (both sides
+        // are non-negative), so the control takes no square roots.
+        const double floor_e = a.noise_floor * kFltEps;
+        const double floor2 = floor_e * floor_e * syy;
 #pragma unroll
         for (int k = 0; k < P; ++k) {
             const double gk = gr[k];
@@ -418,7 +421,7 @@ __device__ __forceinline__ bool lm_plan(const FitArgs &a, const XConst &xc, doub
                         (s.p[k] == a.upper[k] && gk > 0.0);
             if (!active[k]) {
                 gnorm = fmax(gnorm, fabs(gk));
-                at_floor = at_floor && fabs(gk) <= floor_g * sqrt(fmax(A[k * (k + 1) / 2 + k], 0.0));
+                at_floor = at_floor && gk * gk <= floor2 * fmax(A[k * (k + 1) / 2 + k], 0.0);
             }
         }
         if (gnorm <= a.gtol || (parity && at_floor)) {

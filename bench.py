@@ -44,9 +44,9 @@ WORKLOAD = "pseudo_voigt_plain: 1M pseudo-Voigt fits, M=512, float32, p0=None, u
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) of the LM kernel per fit, from the committed ncu capture
 # of the same kernel on 100,000 fits (profiles/fit_kernels_pv512_100k.md): 206.48 MB
-# read + 5.46 MB written.  Traffic grows with the fits processed, so the bench scales
+# read + 5.33 MB written.  Traffic grows with the fits processed, so the bench scales
 # it to the launch's fit count.
-TRAFFIC_BYTES_PER_FIT = (206.482944e6 + 5.461760e6) / 100_000
+TRAFFIC_BYTES_PER_FIT = (206.481408e6 + 5.333248e6) / 100_000
 
 
 def parse():
