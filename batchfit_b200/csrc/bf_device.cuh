@@ -194,30 +194,6 @@ template <int G, int KP, int O, int S> struct ReduceLevel {
     }
 };
 
-// The same reduce-scatter with plain float adds (for sums whose rounding does not
-// need compensation).
-template <int G, int KP, int O, int S> struct ReducePlainLevel {
-    __device__ __forceinline__ static void run(const Group<G> &g, float (&v)[KP], int &slot_base) {
-        if constexpr (O >= 1) {
-            if constexpr (S > 1) {
-                const bool up = (g.lane & unsigned(O)) != 0u;
-#pragma unroll
-                for (int i = 0; i < S / 2; ++i) {
-                    const float send = up ? v[i] : v[i + S / 2];
-                    const float keep = up ? v[i + S / 2] : v[i];
-                    v[i] = keep + g.xor_(send, O);
-                }
-                if (up)
-                    slot_base += S / 2;
-                ReducePlainLevel<G, KP, O / 2, S / 2>::run(g, v, slot_base);
-            } else {
-                v[0] += g.xor_(v[0], O);
-                ReducePlainLevel<G, KP, O / 2, 1>::run(g, v, slot_base);
-            }
-        }
-    }
-};
-
 // Number of slots each lane owns after the reduce-scatter, and the lane-bit mask
 // below which owners are replicas (when KP < G).
 template <int G, int KP> struct ReduceShape {
@@ -242,27 +218,6 @@ __device__ __forceinline__ bool reduce_scatter_store(const Group<G> &g, float (&
             finite = finite && isfinite(v);
             if ((g.lane & unsigned(replicas - 1)) == 0u)
                 out[slot_base + i] = v;
-        }
-    }
-    return finite;
-}
-
-// Plain reduce-scatter of KP per-lane partial sums; slot s is written to out[s].
-// Returns whether every reduced slot this lane owns is finite.
-template <int G, int KP>
-__device__ __forceinline__ bool reduce_scatter_store_plain(const Group<G> &g, float (&v)[KP], double *out,
-                                                           int k_used) {
-    int slot_base = 0;
-    ReducePlainLevel<G, KP, G / 2, KP>::run(g, v, slot_base);
-    constexpr int owned = ReduceShape<G, KP>::owned;
-    constexpr int replicas = ReduceShape<G, KP>::replicas;
-    bool finite = true;
-#pragma unroll
-    for (int i = 0; i < owned; ++i) {
-        if (slot_base + i < k_used) {
-            finite = finite && isfinite(v[i]);
-            if ((g.lane & unsigned(replicas - 1)) == 0u)
-                out[slot_base + i] = double(v[i]);
         }
     }
     return finite;

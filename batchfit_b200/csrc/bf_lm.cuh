@@ -73,34 +73,32 @@ template <int MODEL> constexpr int lm_pairs() { return Model<MODEL>::P <= 4 ? 4 
 //
 // Accumulation: the pair accumulators of a lane sum a few pairs naively; the two
 // halves are then added and folded into Kahan pairs for chi2 and J^T r
-// (numerics::add, numerics.hpp:12-18), which enter a two-sum reduce-scatter with
-// their low parts.  J^T r decides where the iteration stops (its error moves the
-// fixed point), so it gets the compensation; J^T J only shapes the step and takes
-// a plain reduce-scatter.  For P <= 4, J^T J is summed in pairs too (2 T
-// registers); the 8-parameter model keeps scalar sums of its 36 J^T J terms, which
-// would not fit the registers twice.
+// (numerics::add, numerics.hpp:12-18).  J^T r decides where the iteration stops
+// (its error moves the fixed point), so its per-lane sums are compensated; J^T J
+// only shapes the step and sums each lane's pairs naively (at most M / 2G points
+// per accumulator).  All of them then enter one two-sum reduce-scatter across the
+// lanes (J^T J with zero low parts), so every cross-lane addition is compensated.
+// For P <= 4, J^T J is summed in pairs too (2 T registers); the 8-parameter model
+// keeps scalar sums of its 36 J^T J terms, which would not fit the registers twice.
 //
-// pass_sums leaves a lane's partial sums in hi/lo (chi2, J^T r; value hi + lo) and
-// aa (J^T J lower triangle); slots past KC and T are zero.
-template <int MODEL, int LANES, bool PAIRED_LOADS, int KCP, int TP>
+// pass_sums leaves a lane's partial sums in hi/lo (value hi + lo): slot 0 chi2,
+// slots 1..P J^T r, slots KC.. the J^T J lower triangle; slots past KC + T are zero.
+template <int MODEL, int LANES, bool PAIRED_LOADS, int KP>
 __device__ __forceinline__ void pass_sums(int lane, const float *xs, const float *ys, int m, const float *p,
-                                          float (&hi)[KCP], float (&lo)[KCP], float (&aa)[TP]) {
+                                          float (&hi)[KP], float (&lo)[KP]) {
     constexpr int P = Model<MODEL>::P;
     constexpr int KC = P + 1;          // chi2 and J^T r
     constexpr int T = P * (P + 1) / 2; // J^T J lower triangle
     constexpr bool kPairedA = P <= 4;
     constexpr int kPairs = lm_pairs<MODEL>();
-    static_assert(KCP >= KC && TP >= T, "slot arrays");
+    static_assert(KP >= KC + T, "slot arrays");
     const auto q = Model<MODEL>::prepare2(p);
     float2 aa2[kPairedA ? T : 1];
 #pragma unroll
-    for (int i = 0; i < KCP; ++i) {
+    for (int i = 0; i < KP; ++i) {
         hi[i] = 0.0f;
         lo[i] = 0.0f;
     }
-#pragma unroll
-    for (int i = 0; i < TP; ++i)
-        aa[i] = 0.0f;
 #pragma unroll
     for (int i = 0; i < (kPairedA ? T : 1); ++i)
         aa2[i] = splat2(0.0f);
@@ -137,8 +135,8 @@ __device__ __forceinline__ void pass_sums(int lane, const float *xs, const float
                 if constexpr (kPairedA) {
                     aa2[t] = fma2(J[k], J[l], aa2[t]);
                 } else {
-                    aa[t] = fmaf(J[k].x, J[l].x, aa[t]);
-                    aa[t] = fmaf(J[k].y, J[l].y, aa[t]);
+                    hi[KC + t] = fmaf(J[k].x, J[l].x, hi[KC + t]);
+                    hi[KC + t] = fmaf(J[k].y, J[l].y, hi[KC + t]);
                 }
             }
         }
@@ -189,7 +187,7 @@ __device__ __forceinline__ void pass_sums(int lane, const float *xs, const float
     if constexpr (kPairedA) {
 #pragma unroll
         for (int t = 0; t < T; ++t)
-            aa[t] = __fadd_rn(aa2[t].x, aa2[t].y);
+            hi[KC + t] = __fadd_rn(aa2[t].x, aa2[t].y);
     }
 }
 
@@ -199,15 +197,11 @@ __device__ __forceinline__ void pass_sums(int lane, const float *xs, const float
 template <int MODEL, int G, bool PAIRED_LOADS>
 __device__ __forceinline__ bool lm_pass(const Group<G> &g, const float *xs, const float *ys, int m,
                                         const float *p, double *state) {
-    constexpr int P = Model<MODEL>::P;
-    constexpr int KC = P + 1;
-    constexpr int KCP = reduce_slots(KC, G);
-    constexpr int T = P * (P + 1) / 2;
-    constexpr int TP = reduce_slots(T, G);
-    float hi[KCP], lo[KCP], aa[TP];
-    pass_sums<MODEL, G, PAIRED_LOADS>(int(g.lane), xs, ys, m, p, hi, lo, aa);
-    bool finite = reduce_scatter_store<G, KCP>(g, hi, lo, state, KC);
-    finite = reduce_scatter_store_plain<G, TP>(g, aa, state + KC, T) && finite;
+    constexpr int K = Layout<MODEL>::K;
+    constexpr int KP = reduce_slots(K, G);
+    float hi[KP], lo[KP];
+    pass_sums<MODEL, G, PAIRED_LOADS>(int(g.lane), xs, ys, m, p, hi, lo);
+    bool finite = reduce_scatter_store<G, KP>(g, hi, lo, state, K);
     finite = g.all(finite);
     g.sync();
     return finite;

@@ -46,18 +46,13 @@ template <int MODEL> struct CtaShared {
 template <int MODEL, bool PAIRED_LOADS>
 __device__ __forceinline__ bool lm_pass_cta(const float *x, const float *row, int m, const float *p,
                                             double *state, CtaShared<MODEL> &sh) {
-    constexpr int P = Model<MODEL>::P;
     constexpr int K = Layout<MODEL>::K;
-    constexpr int KC = P + 1;
-    constexpr int KCP = reduce_slots(KC, 32);
-    constexpr int T = P * (P + 1) / 2;
-    constexpr int TP = reduce_slots(T, 32);
+    constexpr int KP = reduce_slots(K, 32);
     const Group<32> g;
-    float hi[KCP], lo[KCP], aa[TP];
-    pass_sums<MODEL, kCtaThreads, PAIRED_LOADS>(int(threadIdx.x), x, row, m, p, hi, lo, aa);
+    float hi[KP], lo[KP];
+    pass_sums<MODEL, kCtaThreads, PAIRED_LOADS>(int(threadIdx.x), x, row, m, p, hi, lo);
     double *mine = sh.warp_part[threadIdx.x / 32];
-    bool finite = reduce_scatter_store<32, KCP>(g, hi, lo, mine, KC);
-    finite = reduce_scatter_store_plain<32, TP>(g, aa, mine + KC, T) && finite;
+    bool finite = reduce_scatter_store<32, KP>(g, hi, lo, mine, K);
     finite = __syncthreads_and(finite);
     for (int t = int(threadIdx.x); t < K; t += kCtaThreads) {
         double v = 0.0;
