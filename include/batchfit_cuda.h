@@ -163,8 +163,9 @@ int bf_cuda_last_timing(bf_cuda_context *ctx, bf_cuda_timing *out);
 int bf_cuda_host_alloc(size_t bytes, void **out);
 int bf_cuda_host_free(void *ptr);
 
-/* Largest M bf_cuda_fit takes for `model`.  Spectra that do not fit the group
- * kernels' shared-memory layouts run one CTA (128 threads) per fit, reading x and y
+/* Largest M bf_cuda_fit takes for `model`.  With group_lanes 0, spectra of 6,144
+ * points or more, and any that do not fit the group kernels' shared-memory layouts,
+ * run one CTA (128 threads) per fit, reading x and y
  * through L2, with a long-spectrum guess; they take float32 y. */
 uint32_t bf_cuda_max_points(int32_t model);
 
