@@ -218,6 +218,128 @@ __device__ __forceinline__ bool scan_smoothed(const Group<G> &g, const S &s, F &
     return finite;
 }
 
+// ------------------------------------------------------- chunked sweep --
+// The same sweep over a staged row in 4-sample chunks.  Chunk c (samples 4c..4c+3)
+// goes to group lane c mod G at step c / G; that lane also reads chunk c-1 and
+// tests samples 4c-2..4c+1, whose smoothed values and smoothed neighbours need
+// samples 4c-4..4c+3 only: two 16-byte reads a step, no shuffles.  Chunks
+// 0..m/4 cover every interior sample.  The row must be 16-byte aligned with
+// round_up(m, 4) floats.
+__host__ __device__ inline int chunk_steps(int m, int lanes) { return (m / 4 + lanes) / lanes; }
+// Candidate-bit words per lane: 4 bits a step.
+__host__ __device__ inline int chunk_words(int m, int lanes) { return (chunk_steps(m, lanes) + 7) / 8; }
+// Sample tested as bit b of a lane's candidate bits.
+__device__ __forceinline__ int chunk_sample(int lane, int b, int lanes) {
+    return 4 * (lane + (b >> 2) * lanes) - 2 + (b & 3);
+}
+
+// One step of the chunked sweep for chunk c: cv[t] is the smoothed value of sample
+// j = 4c-2+t when j is an interior smoothed local maximum (v > left, v >= right;
+// initial_guess.hpp:173-174), else 0 (a value that never beats a height >= 0).
+// `fin` accumulates whether the chunk's own samples are finite.  EDGE: the step
+// may touch sample 0, sample m-1 or samples past the row (masked, unsmoothed ends).
+template <bool EDGE, bool SUB>
+__device__ __forceinline__ void chunk_step(const float4 *row, int m, float level, int c, float (&cv)[4], bool &fin) {
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const int j0 = 4 * c - 4;
+    const float4 a = !EDGE || (c >= 1 && j0 < m) ? row[c - 1] : zero;
+    const float4 b = !EDGE || j0 + 4 < m ? row[c] : zero;
+    float s[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}; // samples 4c-4+i
+    if constexpr (SUB) {
+        // The signal of a baseline-only model, y - level (Signal::raw), two at a time.
+#pragma unroll
+        for (int i = 0; i < 8; i += 2) {
+            const float2 d = sub2(make_float2(s[i], s[i + 1]), splat2(level));
+            s[i] = d.x;
+            s[i + 1] = d.y;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (EDGE && j0 + i >= m)
+            s[i] = 0.0f; // the padding of the last chunk is not data
+        if (i >= 4)
+            fin = fin && fabsf(s[i]) <= 3.40282347e+38f;
+    }
+    // 0.25*s and 0.5*s of every sample, two samples per instruction.
+    float q[8], h[8];
+#pragma unroll
+    for (int i = 0; i < 8; i += 2) {
+        const float2 p = make_float2(s[i], s[i + 1]);
+        const float2 pq = mul2(splat2(0.25f), p), ph = mul2(splat2(0.5f), p);
+        q[i] = pq.x;
+        q[i + 1] = pq.y;
+        h[i] = ph.x;
+        h[i + 1] = ph.y;
+    }
+    float v[6]; // smoothed samples 4c-3..4c+2, summed in detail::smooth's order
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+        v[t] = radd(radd(q[t], h[t + 1]), q[t + 2]);
+        if (EDGE && (j0 + 1 + t == 0 || j0 + 1 + t == m - 1))
+            v[t] = s[t + 1];
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        bool peak = v[t + 1] > v[t] && v[t + 1] >= v[t + 2];
+        if (EDGE)
+            peak = peak && j0 + 2 + t >= 1 && j0 + 2 + t <= m - 2;
+        cv[t] = peak ? v[t + 1] : 0.0f;
+    }
+}
+
+// Tallest smoothed local maximum of the group lane's chunks (value and first
+// index; index m when no positive one) and, with BITS, the lane's candidate bits
+// (positive smoothed local maxima, bit 4k+t for sample 4(lane+kG)-2+t, words at
+// bits[w*G]).  SUB: the row holds y and the signal is y - level.  Returns whether
+// the lane's signal samples are finite.
+template <int G, bool BITS, bool SUB>
+__device__ __forceinline__ bool chunk_sweep(const Group<G> &g, const float *signal, int m, float level,
+                                            float &height, int &first, unsigned *bits) {
+    const float4 *row = reinterpret_cast<const float4 *>(signal);
+    const int steps = chunk_steps(m, G);
+    bool fin = true;
+    height = 0.0f;
+    int best = -1;
+    unsigned word = 0;
+    for (int k = 0; k < steps; ++k) {
+        const int c = int(g.lane) + k * G;
+        float cv[4];
+        // The same for every lane of the warp: no lane's step touches an end.
+        if (k > 0 && 4 * (k * G + G) < m)
+            chunk_step<false, SUB>(row, m, level, c, cv, fin);
+        else
+            chunk_step<true, SUB>(row, m, level, c, cv, fin);
+        const float top = fmaxf(fmaxf(cv[0], cv[1]), fmaxf(cv[2], cv[3]));
+        if (top > height) {
+            height = top;
+            best = k;
+        }
+        if constexpr (BITS) {
+            word |= (unsigned(cv[0] > 0.0f) | unsigned(cv[1] > 0.0f) << 1 | unsigned(cv[2] > 0.0f) << 2 |
+                     unsigned(cv[3] > 0.0f) << 3)
+                    << (4 * (k & 7));
+            if ((k & 7) == 7 || k + 1 == steps) {
+                bits[(k >> 3) * G + int(g.lane)] = word;
+                word = 0;
+            }
+        }
+    }
+    first = m;
+    if (best >= 0) {
+        // The first sample of the best step that reaches the height.
+        const int c = int(g.lane) + best * G;
+        float cv[4];
+        bool unused = true;
+        chunk_step<true, SUB>(row, m, level, c, cv, unused);
+#pragma unroll
+        for (int t = 3; t >= 0; --t)
+            if (cv[t] == height)
+                first = 4 * c - 2 + t;
+    }
+    return fin;
+}
+
 // Group argmax of (value, index): larger value wins, ties go to the smaller index.
 template <int G> __device__ __forceinline__ void argmax_pair(const Group<G> &g, float &v, int &i) {
 #pragma unroll
@@ -322,8 +444,10 @@ __host__ __device__ inline int lane_samples(int m, int lane, int lanes) {
 }
 // Scratch words of the second-peak search: four block arrays, then one candidate
 // bit per interior sample (lane-wise words, word-major).
+// (Either sweep's layout: the lane-interleaved or the chunked one.)
 __host__ __device__ inline int second_peak_words(int m, int lanes) {
-    return 4 * walk_blocks(m) + lanes * ((lane_samples(m, 0, lanes) + 31) / 32);
+    const int interleaved = (lane_samples(m, 0, lanes) + 31) / 32, chunked = chunk_words(m, lanes);
+    return 4 * walk_blocks(m) + lanes * (interleaved > chunked ? interleaved : chunked);
 }
 template <int G, class S>
 __device__ void block_extrema(const Group<G> &g, const S &s, float *bmin, float *bmax) {
@@ -523,9 +647,12 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
     const float noise = rmul(1.4826f, noise_median);
     if (!isfinite(noise))
         return kGuessInvalid;
-    if constexpr (PRE) {
-        // ys is this group's own staged, 16-byte aligned copy of the row (padded to
-        // a multiple of 4 floats, as is xs): overwrite it with the signal.
+    // PRE: ys is this group's own staged, 16-byte aligned copy of the row (padded to
+    // a multiple of 4 floats, as is xs).  The two-Lorentzian's signal needs x and is
+    // read many times by the second-peak search: it overwrites the row once.  The
+    // other models' signal is y - level, formed wherever a sample is read.
+    constexpr bool overwrite = PRE && paired;
+    if constexpr (overwrite) {
         const Signal<MODEL> raw{xs, ys, level, slope, xc.left_x, m};
         float4 *row = reinterpret_cast<float4 *>(const_cast<float *>(ys));
         const float4 *xq = reinterpret_cast<const float4 *>(xs);
@@ -537,7 +664,7 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         }
         g.sync();
     }
-    const Signal<MODEL, PRE> s{xs, ys, level, slope, xc.left_x, m};
+    const Signal<MODEL, overwrite> s{xs, ys, level, slope, xc.left_x, m};
     // Tallest smoothed local maximum (initial_guess.hpp:170-179).  The same sweep
     // checks that every signal sample is finite (initial_guess.hpp:158-162); both
     // failures end in invalid_input, so their order does not matter.  For the
@@ -548,22 +675,27 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
     float height = 0.0f;
     int first = m;
     [[maybe_unused]] unsigned *cand_bits = reinterpret_cast<unsigned *>(scratch + 4 * walk_blocks(m));
-    [[maybe_unused]] unsigned word = 0;
-    const bool signal_finite = scan_smoothed<G>(g, s, [&](int j, float v, float left, float right) {
-        const bool peak = v > 0.0f && v > left && v >= right;
-        if (peak && v > height) {
-            height = v;
-            first = j;
-        }
-        if constexpr (paired) {
-            const int k = int(unsigned(j - 1 - int(g.lane)) / G);
-            word |= unsigned(peak) << (k & 31);
-            if ((k & 31) == 31 || j + G + 1 >= m) {
-                cand_bits[(k >> 5) * G + int(g.lane)] = word;
-                word = 0;
+    bool signal_finite;
+    if constexpr (PRE) {
+        signal_finite = chunk_sweep<G, paired, !overwrite>(g, ys, m, level, height, first, cand_bits);
+    } else {
+        [[maybe_unused]] unsigned word = 0;
+        signal_finite = scan_smoothed<G>(g, s, [&](int j, float v, float left, float right) {
+            const bool peak = v > 0.0f && v > left && v >= right;
+            if (peak && v > height) {
+                height = v;
+                first = j;
             }
-        }
-    });
+            if constexpr (paired) {
+                const int k = int(unsigned(j - 1 - int(g.lane)) / G);
+                word |= unsigned(peak) << (k & 31);
+                if ((k & 31) == 31 || j + G + 1 >= m) {
+                    cand_bits[(k >> 5) * G + int(g.lane)] = word;
+                    word = 0;
+                }
+            }
+        });
+    }
     if (!g.all(signal_finite))
         return kGuessInvalid;
     argmax_pair(g, height, first);
@@ -608,7 +740,9 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
             const int bins = idx > first ? idx - first : first - idx;
             return !(bins < 3 || fabsf(rsub(xs[idx], primary.center)) < separation);
         };
-        const int words = (lane_samples(m, int(g.lane), G) + 31) >> 5;
+        const int words = PRE ? chunk_words(m, G) : (lane_samples(m, int(g.lane), G) + 31) >> 5;
+        // Sample of bit b of this lane's candidate words (the layout of the sweep used).
+        auto cand_sample = [&](int b) { return PRE ? chunk_sample(int(g.lane), b, G) : 1 + int(g.lane) + b * G; };
         const unsigned *bits = cand_bits + int(g.lane);
         int second = m;
         float v1 = 0.0f, v2 = 0.0f;
@@ -616,7 +750,7 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         for (int w = 0; w < words; ++w) {
             unsigned cand = bits[w * G];
             while (cand) {
-                const int j = 1 + int(g.lane) + (w * 32 + __ffs(cand) - 1) * G;
+                const int j = cand_sample(w * 32 + __ffs(cand) - 1);
                 cand &= cand - 1;
                 const float v = s.smooth_interior(j);
                 if (!(v > v2 || (v == v2 && j < j2)) || !far_enough(j))
@@ -669,7 +803,7 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
                         cand = bits[++cw * G];
                     if (cand == 0)
                         break;
-                    j = 1 + int(g.lane) + (cw * 32 + __ffs(cand) - 1) * G;
+                    j = cand_sample(cw * 32 + __ffs(cand) - 1);
                     cand &= cand - 1;
                     const float v = s.smooth_interior(j);
                     if ((v < cut_v || (v == cut_v && j > cut_j)) && (v > bv || (v == bv && j < bj)) &&

@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(GuessShapeCfg<V>::threads, GuessShapeCfg<V>::m
     for (long long fit = (long long)blockIdx.x * kGroups + gid; fit < n; fit += (long long)gridDim.x * kGroups) {
         bool yfin, flat;
         float syy;
-        stage_fit_row(g, y, y_half, fit, m, vec_ok, ys, yfin, flat, syy);
+        stage_fit_row<G, false>(g, y, y_half, fit, m, vec_ok, ys, yfin, flat, syy); // the guess needs only yfin
         float p[P];
         const int gs = initial_guess<MODEL, G, V, true>(g, cx, xs, ys, yfin, scratch, p);
 #pragma unroll

@@ -656,9 +656,9 @@ __device__ __forceinline__ void write_information(const Grp &g, const FitArgs &a
 }
 
 // Stage one fit-major y row into shared memory (kStore) or only scan it; reports
-// finiteness, flatness (every value equal to y[0]) and sum(y^2), with the same
-// arithmetic either way.
-template <int G, bool kStore = true>
+// finiteness and, with kSums, flatness (every value equal to y[0]) and sum(y^2),
+// with the same arithmetic either way (without kSums: flat false, syy 0).
+template <int G, bool kStore = true, bool kSums = true>
 __device__ __forceinline__ void stage_row(const Group<G> &g, const float *row, int m, bool vec_ok, float *ys,
                                           bool &yfin, bool &flat, float &syy) {
     const float y0 = __ldg(row);
@@ -672,8 +672,10 @@ __device__ __forceinline__ void stage_row(const Group<G> &g, const float *row, i
             if constexpr (kStore)
                 reinterpret_cast<float4 *>(ys)[v] = t;
             yfin = yfin && isfinite(t.x) && isfinite(t.y) && isfinite(t.z) && isfinite(t.w);
-            flat = flat && t.x == y0 && t.y == y0 && t.z == y0 && t.w == y0;
-            syy = fmaf(t.x, t.x, fmaf(t.y, t.y, fmaf(t.z, t.z, fmaf(t.w, t.w, syy))));
+            if constexpr (kSums) {
+                flat = flat && t.x == y0 && t.y == y0 && t.z == y0 && t.w == y0;
+                syy = fmaf(t.x, t.x, fmaf(t.y, t.y, fmaf(t.z, t.z, fmaf(t.w, t.w, syy))));
+            }
         }
     } else {
         for (int j = int(g.lane); j < m; j += G) {
@@ -681,22 +683,28 @@ __device__ __forceinline__ void stage_row(const Group<G> &g, const float *row, i
             if constexpr (kStore)
                 ys[j] = t;
             yfin = yfin && isfinite(t);
-            flat = flat && t == y0;
-            syy = fmaf(t, t, syy);
+            if constexpr (kSums) {
+                flat = flat && t == y0;
+                syy = fmaf(t, t, syy);
+            }
         }
     }
     yfin = g.all(yfin);
-    flat = g.all(flat);
+    if constexpr (kSums) {
+        flat = g.all(flat);
 #pragma unroll
-    for (int o = G / 2; o >= 1; o >>= 1)
-        syy += g.xor_(syy, o);
+        for (int o = G / 2; o >= 1; o >>= 1)
+            syy += g.xor_(syy, o);
+    } else {
+        flat = false;
+    }
     g.sync();
 }
 
 // A row of y stored as IEEE binary16 (opt-in half-precision storage), converted
 // exactly to float32 while it is staged, with stage_row's accumulations in the same
 // order: a fit of half-precision y equals the fit of the same values given as float.
-template <int G>
+template <int G, bool kSums = true>
 __device__ __forceinline__ void stage_row_half(const Group<G> &g, const __half *row, int m, bool vec_ok, float *ys,
                                                bool &yfin, bool &flat, float &syy) {
     const float y0 = __half2float(row[0]);
@@ -712,23 +720,31 @@ __device__ __forceinline__ void stage_row_half(const Group<G> &g, const __half *
             const float4 t = make_float4(a.x, a.y, b.x, b.y);
             reinterpret_cast<float4 *>(ys)[v] = t;
             yfin = yfin && isfinite(t.x) && isfinite(t.y) && isfinite(t.z) && isfinite(t.w);
-            flat = flat && t.x == y0 && t.y == y0 && t.z == y0 && t.w == y0;
-            syy = fmaf(t.x, t.x, fmaf(t.y, t.y, fmaf(t.z, t.z, fmaf(t.w, t.w, syy))));
+            if constexpr (kSums) {
+                flat = flat && t.x == y0 && t.y == y0 && t.z == y0 && t.w == y0;
+                syy = fmaf(t.x, t.x, fmaf(t.y, t.y, fmaf(t.z, t.z, fmaf(t.w, t.w, syy))));
+            }
         }
     } else {
         for (int j = int(g.lane); j < m; j += G) {
             const float t = __half2float(row[j]);
             ys[j] = t;
             yfin = yfin && isfinite(t);
-            flat = flat && t == y0;
-            syy = fmaf(t, t, syy);
+            if constexpr (kSums) {
+                flat = flat && t == y0;
+                syy = fmaf(t, t, syy);
+            }
         }
     }
     yfin = g.all(yfin);
-    flat = g.all(flat);
+    if constexpr (kSums) {
+        flat = g.all(flat);
 #pragma unroll
-    for (int o = G / 2; o >= 1; o >>= 1)
-        syy += g.xor_(syy, o);
+        for (int o = G / 2; o >= 1; o >>= 1)
+            syy += g.xor_(syy, o);
+    } else {
+        flat = false;
+    }
     g.sync();
 }
 
@@ -738,13 +754,13 @@ __device__ __forceinline__ bool rows_vectorisable(const float *y, int m, bool y_
 }
 
 // Stage row `fit` of y (float32, or binary16 when y_half) into shared memory.
-template <int G>
+template <int G, bool kSums = true>
 __device__ __forceinline__ void stage_fit_row(const Group<G> &g, const float *y, bool y_half, long long fit, int m,
                                               bool vec_ok, float *ys, bool &yfin, bool &flat, float &syy) {
     if (y_half)
-        stage_row_half<G>(g, reinterpret_cast<const __half *>(y) + fit * m, m, vec_ok, ys, yfin, flat, syy);
+        stage_row_half<G, kSums>(g, reinterpret_cast<const __half *>(y) + fit * m, m, vec_ok, ys, yfin, flat, syy);
     else
-        stage_row<G>(g, y + fit * m, m, vec_ok, ys, yfin, flat, syy);
+        stage_row<G, true, kSums>(g, y + fit * m, m, vec_ok, ys, yfin, flat, syy);
 }
 
 // Covariance of one finished fit from the information matrix the LM kernel left in
