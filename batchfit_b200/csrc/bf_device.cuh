@@ -57,30 +57,32 @@ __device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
+// a / 2 exactly as the division rounds it: a / 2 and a * 0.5 are the same real
+// number, so their correctly rounded results are equal (subnormals included).
+__device__ __forceinline__ float rhalf(float a) { return __fmul_rn(a, 0.5f); }
 
 // std::midpoint for float (C++20 [numeric.ops.midpoint]).
 __device__ __forceinline__ float midpoint_rn(float a, float b) {
     const float lo = 1.17549435e-38f * 2.0f, hi = 3.40282347e+38f / 2.0f;
     const float aa = fabsf(a), ab = fabsf(b);
     if (aa <= hi && ab <= hi)
-        return rdiv(radd(a, b), 2.0f);
+        return rhalf(radd(a, b));
     if (aa < lo)
-        return radd(a, rdiv(b, 2.0f));
+        return radd(a, rhalf(b));
     if (ab < lo)
-        return radd(rdiv(a, 2.0f), b);
-    return radd(rdiv(a, 2.0f), rdiv(b, 2.0f));
+        return radd(rhalf(a), b);
+    return radd(rhalf(a), rhalf(b));
 }
 
 // std::lerp for float as libstdc++ evaluates it (C++20 [c.math.lerp]).
+// Both formulas are evaluated and the result selected, so that the groups of a warp
+// do not split on the branches.
 __device__ __forceinline__ float lerp_rn(float a, float b, float t) {
-    if ((a <= 0.0f && b >= 0.0f) || (a >= 0.0f && b <= 0.0f))
-        return radd(rmul(t, b), rmul(rsub(1.0f, t), a));
-    if (t == 1.0f)
-        return b;
+    const bool straddle = (a <= 0.0f && b >= 0.0f) || (a >= 0.0f && b <= 0.0f);
+    const float across = radd(rmul(t, b), rmul(rsub(1.0f, t), a));
     const float v = radd(a, rmul(t, rsub(b, a)));
-    if ((t > 1.0f) == (b > a))
-        return b < v ? v : b;
-    return b > v ? v : b;
+    const float bounded = (t > 1.0f) == (b > a) ? (b < v ? v : b) : (b > v ? v : b);
+    return straddle ? across : (t == 1.0f ? b : bounded);
 }
 
 // std::min / std::max argument semantics (ties keep the first argument).

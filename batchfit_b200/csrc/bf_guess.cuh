@@ -105,6 +105,21 @@ template <int G, int V> __device__ __forceinline__ void reg_merge(const Group<G>
         reg_stage<G, V>(g, v, N, j, true);
 }
 
+// Store a blocked run (lane l holds elements l*V .. l*V+V-1) to a 16-byte aligned
+// buffer, 16 bytes at a time when V allows.
+template <int G, int V> __device__ __forceinline__ void store_run(const Group<G> &g, const float (&v)[V], float *out) {
+    if constexpr (V % 4 == 0) {
+        float4 *o = reinterpret_cast<float4 *>(out + int(g.lane) * V);
+#pragma unroll
+        for (int i = 0; i < V; i += 4)
+            o[i / 4] = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < V; ++i)
+            out[int(g.lane) * V + i] = v[i];
+    }
+}
+
 // Median of the union of sorted a[0..n) and b[0..n) (2n values, an even count):
 // the midpoint of its n-1-th and n-th smallest.  One merge-path search splits off
 // the n smallest (i from a, n-i from b); the n-1-th is the larger of the last ones
@@ -367,7 +382,7 @@ __device__ PeakFeature find_peak(const Group<G> &g, const S &s, const float *xs,
     r.amplitude = s.at(index);
     if (!(r.amplitude > 0.0f))
         return r;
-    const float half = rdiv(r.amplitude, 2.0f);
+    const float half = rhalf(r.amplitude);
     // while (left > begin && signal[left] > half) --left;
     int left = begin;
     for (int top = index - 1; top >= begin; top -= G) {
@@ -404,14 +419,22 @@ __device__ PeakFeature find_peak(const Group<G> &g, const S &s, const float *xs,
     const int high_limit = has_right ? right - 1 : end;
     low = low < low_limit ? low_limit : low;
     high = high_limit < high ? high_limit : high;
+    // Weighted centre over j = low..high, a window of at most 5 samples around the
+    // index: a fixed 5-step loop with inactive steps selected away, so that the
+    // groups of a warp run it together.
     float total = 0.0f;
     r.center = xs[index];
-    for (int j = low; j <= high; ++j) {
-        const float w = rdiv(smax(0.0f, s.at(j)), r.amplitude);
-        if (w > 0.0f) {
-            total = radd(total, w);
-            r.center = lerp_rn(r.center, xs[j], rdiv(w, total));
-        }
+#pragma unroll
+    for (int d = -2; d <= 2; ++d) {
+        const int j = index + d;
+        const bool active = j >= low && j <= high;
+        const int jj = active ? j : index;
+        const float w = rdiv(smax(0.0f, s.at(jj)), r.amplitude);
+        const bool take = active && w > 0.0f;
+        const float sum = radd(total, w);
+        const float moved = lerp_rn(r.center, xs[jj], rdiv(take ? w : 0.0f, take ? sum : 1.0f));
+        total = take ? sum : total;
+        r.center = take ? moved : r.center;
     }
     auto crossing = [&](int a, int b) {
         const float den = rsub(s.at(b), s.at(a));
@@ -565,19 +588,18 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         // the union median by a merge-path search over the two sorted runs.
         constexpr int N = G * V;
         float lv[V], rv[V];
+        // Any placement sorts: lane l reads samples l, l+G, ... (consecutive lanes,
+        // consecutive banks); the sorted values come out blocked, V per lane.
 #pragma unroll
         for (int i = 0; i < V; ++i) {
-            const int e = int(g.lane) * V + i;
+            const int e = i * G + int(g.lane);
             lv[i] = e < count ? ys[e] : __int_as_float(0x7f800000);
             rv[i] = e < count ? ys[m - count + e] : __int_as_float(0x7f800000);
         }
         reg_sort<G, V>(g, lv);
         reg_sort<G, V>(g, rv);
-#pragma unroll
-        for (int i = 0; i < V; ++i) {
-            scratch[int(g.lane) * V + i] = lv[i];
-            scratch[N + int(g.lane) * V + i] = rv[i];
-        }
+        store_run<G, V>(g, lv, scratch);
+        store_run<G, V>(g, rv, scratch + N);
         g.sync();
         left_level = sorted_median(scratch, count);
         right_level = sorted_median(scratch + N, count);
@@ -595,11 +617,8 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         }
         reg_merge<G, V>(g, lv);
         reg_merge<G, V>(g, rv);
-#pragma unroll
-        for (int i = 0; i < V; ++i) {
-            scratch[int(g.lane) * V + i] = lv[i];
-            scratch[N + int(g.lane) * V + i] = rv[i];
-        }
+        store_run<G, V>(g, lv, scratch);
+        store_run<G, V>(g, rv, scratch + N);
         g.sync();
         noise_median = union_median(scratch, scratch + N, count);
         g.sync();
@@ -711,7 +730,7 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
         if constexpr (MODEL == kGaussian)
             out[2] = rdiv(primary.width, 2.354820045030949382f);
         else if constexpr (MODEL == kLorentzian)
-            out[2] = rdiv(primary.width, 2.0f);
+            out[2] = rhalf(primary.width);
         else {
             out[2] = primary.width;
             out[3] = 0.5f;
@@ -895,10 +914,10 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
             return kGuessInsufficient;
         out[0] = primary.amplitude;
         out[1] = primary.center;
-        out[2] = rdiv(primary.width, 2.0f);
+        out[2] = rhalf(primary.width);
         out[3] = secondary.amplitude;
         out[4] = secondary.center;
-        out[5] = rdiv(secondary.width, 2.0f);
+        out[5] = rhalf(secondary.width);
         out[6] = rsub(left_level, rmul(slope, xc.left_x));
         out[7] = slope;
     }
