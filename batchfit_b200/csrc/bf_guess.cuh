@@ -7,6 +7,8 @@
 // keep the reference's tie rules (first maximum / first minimum in index order).
 #pragma once
 
+#include <type_traits>
+
 #include "bf_device.cuh"
 #include "bf_models.cuh"
 
@@ -317,14 +319,9 @@ __device__ __forceinline__ bool chunk_sweep(const Group<G> &g, const float *sign
     height = 0.0f;
     int best = -1;
     unsigned word = 0;
-    for (int k = 0; k < steps; ++k) {
-        const int c = int(g.lane) + k * G;
+    auto visit = [&](auto edge, int k) {
         float cv[4];
-        // The same for every lane of the warp: no lane's step touches an end.
-        if (k > 0 && 4 * (k * G + G) < m)
-            chunk_step<false, SUB>(row, m, level, c, cv, fin);
-        else
-            chunk_step<true, SUB>(row, m, level, c, cv, fin);
+        chunk_step<decltype(edge)::value, SUB>(row, m, level, int(g.lane) + k * G, cv, fin);
         const float top = fmaxf(fmaxf(cv[0], cv[1]), fmaxf(cv[2], cv[3]));
         if (top > height) {
             height = top;
@@ -339,7 +336,17 @@ __device__ __forceinline__ bool chunk_sweep(const Group<G> &g, const float *sign
                 word = 0;
             }
         }
-    }
+    };
+    // Steps 1 <= k < inner touch neither end of the row for any lane (4G(k+1) < m):
+    // those run branch-free, two per loop turn; the first and the last take the
+    // masked step.
+    const int inner = min(steps, (m - 1) / (4 * G));
+    visit(std::true_type{}, 0);
+#pragma unroll 2
+    for (int k = 1; k < inner; ++k)
+        visit(std::false_type{}, k);
+    for (int k = inner > 1 ? inner : 1; k < steps; ++k)
+        visit(std::true_type{}, k);
     first = m;
     if (best >= 0) {
         // The first sample of the best step that reaches the height.
@@ -419,33 +426,50 @@ __device__ PeakFeature find_peak(const Group<G> &g, const S &s, const float *xs,
     const int high_limit = has_right ? right - 1 : end;
     low = low < low_limit ? low_limit : low;
     high = high_limit < high ? high_limit : high;
-    // Weighted centre over j = low..high, a window of at most 5 samples around the
-    // index: a fixed 5-step loop with inactive steps selected away, so that the
-    // groups of a warp run it together.
-    float total = 0.0f;
+    // Weighted centre over j = low..high (a window of at most 5 samples around the
+    // index), detail::peak's loop: total += w; centre = lerp(centre, x[j], w/total)
+    // for every w = max(0, s[j]) / amplitude > 0.  The divisions run side by side:
+    // lane d takes sample index-2+d, every lane forms the running totals in the
+    // window's order, and lane d divides its weight by its own running total.  Only
+    // the lerp chain stays sequential.  Operations and order are the loop's.
+    const int lane = int(g.lane);
+    const int jl = index - 2 + lane;
+    const bool mine = lane < 5 && jl >= low && jl <= high;
+    const float w_own = mine ? rdiv(smax(0.0f, s.at(mine ? jl : index)), r.amplitude) : 0.0f;
+    float w[5];
+#pragma unroll
+    for (int d = 0; d < 5; ++d)
+        w[d] = g.bcast(w_own, d);
+    float total = 0.0f, own_total = 1.0f;
+#pragma unroll
+    for (int d = 0; d < 5; ++d) {
+        if (w[d] > 0.0f)
+            total = radd(total, w[d]);
+        if (d == lane)
+            own_total = total;
+    }
+    const float q_own = w_own > 0.0f ? rdiv(w_own, own_total) : 0.0f;
     r.center = xs[index];
 #pragma unroll
-    for (int d = -2; d <= 2; ++d) {
-        const int j = index + d;
-        const bool active = j >= low && j <= high;
-        const int jj = active ? j : index;
-        const float w = rdiv(smax(0.0f, s.at(jj)), r.amplitude);
-        const bool take = active && w > 0.0f;
-        const float sum = radd(total, w);
-        const float moved = lerp_rn(r.center, xs[jj], rdiv(take ? w : 0.0f, take ? sum : 1.0f));
-        total = take ? sum : total;
-        r.center = take ? moved : r.center;
+    for (int d = 0; d < 5; ++d) {
+        const float q = g.bcast(q_own, d);
+        const float xd = xs[w[d] > 0.0f ? index - 2 + d : index]; // in the window when taken
+        if (w[d] > 0.0f)
+            r.center = lerp_rn(r.center, xd, q);
     }
-    auto crossing = [&](int a, int b) {
+    // Both half-height crossings at once: lane 0 the left one, lane 1 the right one.
+    float cross = __int_as_float(0x7fffffff);
+    if ((lane == 0 && has_left) || (lane == 1 && has_right)) {
+        const int a = lane == 0 ? left : right - 1, b = a + 1;
         const float den = rsub(s.at(b), s.at(a));
-        if (!isfinite(den) || den == 0.0f)
-            return __int_as_float(0x7fffffff);
-        return lerp_rn(xs[a], xs[b], rdiv(rsub(half, s.at(a)), den));
-    };
+        if (isfinite(den) && den != 0.0f)
+            cross = lerp_rn(xs[a], xs[b], rdiv(rsub(half, s.at(a)), den));
+    }
+    const float cross_left = g.bcast(cross, 0), cross_right = g.bcast(cross, 1);
     if (has_left)
-        r.left_radius = rsub(r.center, crossing(left, left + 1));
+        r.left_radius = rsub(r.center, cross_left);
     if (has_right)
-        r.right_radius = rsub(crossing(right - 1, right), r.center);
+        r.right_radius = rsub(cross_right, r.center);
     if (!has_left)
         r.left_radius = r.right_radius;
     if (!has_right)
