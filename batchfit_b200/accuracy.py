@@ -76,9 +76,14 @@ def chi2_errors(got, ref):
 
 
 def summarize(model, x, y, got_params, got_status, got_chi2, ref_params, ref_status, ref_chi2,
-              param_tol=1e-4, chi2_tol=1e-5, x64=False):
+              param_tol=1e-4, chi2_tol=1e-5, x64=False, bounds=None):
     """Accuracy summary of a float32 result against the float64 oracle.  x64 adds
-    the definite-status agreement and the float32-equivalence fraction."""
+    the definite-status agreement and the float32-equivalence fraction; with
+    `bounds` (lower, upper) it also gives, over the oracle-converged fits, the
+    two float32 bounds relative to the parameter errors' denominators: the
+    first-order fixed-point bound (``perturbation_bound``), with the fraction
+    within tolerance among the fits where it is below param_tol, and the chi2
+    resolution (``resolution_bound``), with the same split."""
     agree = np.asarray(got_status) == np.asarray(ref_status)
     converged = agree & np.isin(np.asarray(ref_status), (0, 5))
     pe = param_errors(model, x, y, got_params, ref_params)
@@ -97,6 +102,23 @@ def summarize(model, x, y, got_params, got_status, got_chi2, ref_params, ref_sta
         extra = {"status_agreement_definite": float(agree[definite].mean()) if definite.any() else 1.0,
                  "definite_fraction": float(definite.mean()) if n else 1.0,
                  "within_or_equivalent_fraction": float(equivalent[converged].sum() / conv)}
+        if bounds is not None:
+            ref_conv = np.isin(np.asarray(ref_status), (0, 5))
+            den = floors(model, x, y)
+            refp = np.asarray(ref_params, np.float64)
+            rel = {"first_order": np.full(n, np.inf), "chi2_resolution": np.full(n, np.inf)}
+            for i in np.where(ref_conv)[0]:
+                yi = np.asarray(y[i], np.float64)
+                d = np.maximum(np.abs(refp[i]), den[i])
+                for name, fn in (("first_order", perturbation_bound), ("chi2_resolution", resolution_bound)):
+                    b = fn(model, x, yi, refp[i], bounds[0], bounds[1])
+                    with np.errstate(divide="ignore", invalid="ignore"):
+                        rel[name][i] = float(np.max(np.where(b == 0.0, 0.0, b / d)))
+            for name, r in rel.items():
+                small = ref_conv & (r <= param_tol)
+                extra[f"{name}_median"] = float(np.median(r[ref_conv])) if ref_conv.any() else 0.0
+                extra[f"{name}_below_tol_fraction"] = float(small[ref_conv].mean()) if ref_conv.any() else 1.0
+                extra[f"within_tol_where_{name}_below_tol"] = float(within[small].mean()) if small.any() else None
     return {**extra,
         "n": n,
         "status_agreement": float(agree.mean()) if n else 1.0,
@@ -154,6 +176,69 @@ def chi2_error_bound(model, x, y, params):
     f, _ = model_and_jacobian(model, x, params)
     y = np.asarray(y, np.float64)
     return 2.0 * U32 * float(np.sum(np.abs(y - f) * (np.abs(y) + np.abs(f))))
+
+
+def _free(p, lower, upper):
+    free = np.ones(p.size, bool)
+    if lower is not None:
+        free &= p > np.asarray(lower, np.float64)
+    if upper is not None:
+        free &= p < np.asarray(upper, np.float64)
+    return free
+
+
+def perturbation_bound(model, x, y, params, lower=None, upper=None):
+    """First-order bound of how far float32 evaluation moves the fixed point of a
+    gradient-based solver from a float64 minimiser `params`: each residual carries
+    an error of at most u32 (|y| + |f|), the stationarity condition J^T r = 0
+    shifts by J^T of it, and the parameters by (J^T J)^-1 J^T of it:
+    |dp_k| <= sum_i |[(J^T J)^-1 J^T]_ki| u32 (|y_i| + |f_i|), over the free
+    parameters (0 at a bound, inf when J^T J is singular)."""
+    p = np.asarray(params, np.float64)
+    if not np.all(np.isfinite(p)):
+        return np.full(p.size, np.inf)
+    f, J = model_and_jacobian(model, x, p)
+    free = _free(p, lower, upper)
+    out = np.zeros(p.size)
+    if not free.any():
+        return out
+    Jf = J[:, free]
+    try:
+        G = np.linalg.solve(Jf.T @ Jf, Jf.T)
+    except np.linalg.LinAlgError:
+        out[free] = np.inf
+        return out
+    out[free] = np.abs(G) @ (U32 * (np.abs(np.asarray(y, np.float64)) + np.abs(f)))
+    return out
+
+
+def resolution_bound(model, x, y, params, lower=None, upper=None):
+    """Per-parameter float32 resolution at a float64 minimiser `params`: the
+    largest move of parameter k that keeps the Gauss-Newton chi2 within the float32
+    evaluation error of chi2 (``chi2_error_bound``), max |dp_k| subject to
+    dp^T (J^T J) dp <= eps, which is sqrt(eps * [(J^T J)^-1]_kk) over the free
+    parameters (strictly inside their bounds).  Parameters at a bound get 0; a
+    singular J^T J gives inf.  A fit whose bound is below the tolerance is one a
+    float32 solver can pin down to it; above it, float32 cannot order the points
+    that separate the answers."""
+    p = np.asarray(params, np.float64)
+    if not np.all(np.isfinite(p)):
+        return np.full(p.size, np.inf)
+    _, J = model_and_jacobian(model, x, p)
+    eps = chi2_error_bound(model, x, y, p)
+    free = _free(p, lower, upper)
+    out = np.zeros(p.size)
+    if not free.any():
+        return out
+    Jf = J[:, free]
+    try:
+        inv = np.linalg.inv(Jf.T @ Jf)
+    except np.linalg.LinAlgError:
+        out[free] = np.inf
+        return out
+    d = np.diag(inv)
+    out[free] = np.where(d > 0, np.sqrt(eps * np.maximum(d, 0.0)), np.inf)
+    return out
 
 
 def float32_equivalent(model, x, y, got, ref):

@@ -411,9 +411,9 @@ def configs_section(ctx, dev, steps=5, warmup=3):
                              options=pyoracle.make_options(max_iterations=2000, gradient_tolerance=1e-16,
                                                            step_tolerance=1e-16, cost_tolerance=1e-18))
         s = accuracy.summarize(w.model, w.x, w.y[:k], res["params"][:k], res["status"][:k], res["chi2"][:k],
-                               ref.params, ref.status, ref.chi2, x64=True)
+                               ref.params, ref.status, ref.chi2, x64=True, bounds=(w.lower, w.upper))
         s32 = accuracy.summarize(w.model, w.x, w.y[:k], r32.params, r32.status, r32.chi2, ref.params, ref.status,
-                                 ref.chi2, x64=True)
+                                 ref.chi2, x64=True, bounds=(w.lower, w.upper))
         s64 = accuracy.summarize(w.model, w.x, w.y[:k], tight.params, tight.status, tight.chi2, ref.params,
                                  ref.status, ref.chi2)
         codes, counts = np.unique(res["status"], return_counts=True)
@@ -440,6 +440,19 @@ def configs_section(ctx, dev, steps=5, warmup=3):
                          "reference_float32_within_or_float32_equivalent":
                              round(s32["within_or_equivalent_fraction"], 6),
                          "float64_tight_vs_default_within_tol": round(s64["within_tol_fraction"], 6),
+                         "float32_bounds": {
+                             "what": "over the oracle-converged fits, relative to the parameter errors' "
+                                     "denominators: first_order = (J^T J)^-1 J^T of u32 (|y|+|f|), how far float32 "
+                                     "evaluation moves the fixed point J^T r = 0; chi2_resolution = "
+                                     "sqrt(eps (J^T J)^-1_kk), how far parameters move while chi2 stays within its "
+                                     "float32 evaluation error eps",
+                             "first_order_median": s["first_order_median"],
+                             "first_order_below_tol_fraction": round(s["first_order_below_tol_fraction"], 6),
+                             "within_tol_where_first_order_below_tol": s["within_tol_where_first_order_below_tol"],
+                             "reference_float32_within_tol_where_first_order_below_tol":
+                                 s32["within_tol_where_first_order_below_tol"],
+                             "chi2_resolution_median": s["chi2_resolution_median"],
+                             "chi2_resolution_below_tol_fraction": round(s["chi2_resolution_below_tol_fraction"], 6)},
                          "param_tol": 1e-4, "chi2_tol": 1e-5},
         }
         del x_d, y_d, o
@@ -585,7 +598,9 @@ def summary_of(line):
         out["cube"] = {"fits_per_s": round(cube["fits_per_s"]),
                        "status_definite": cube["accuracy"]["status_agreement_definite"],
                        "within_1e-4": cube["accuracy"]["within_tol_fraction"],
-                       "within_or_f32_equivalent": cube["accuracy"]["within_or_float32_equivalent"]}
+                       "within_or_f32_equivalent": cube["accuracy"]["within_or_float32_equivalent"],
+                       "within_where_first_order_bound_small":
+                           cube["accuracy"]["float32_bounds"]["within_tol_where_first_order_below_tol"]}
     mixed = line.get("mixed")
     if mixed:
         out["mixed"] = {"batched_ms": mixed["batched"]["device_ms"], "fixed_ms": mixed["fixed_mapping"]["device_ms"],

@@ -63,3 +63,35 @@ def test_summarize_definite_and_equivalent_fractions(oracle):
     assert s["status_agreement_definite"] == 1.0
     assert s["definite_fraction"] == pytest.approx(2 / 3)
     assert s["within_or_equivalent_fraction"] == 0.5
+
+
+def test_float32_bounds_are_the_extremes_they_claim(oracle):
+    """perturbation_bound is the largest first-order shift of the fixed point over
+    every residual error of size u32 (|y| + |f|) (attained by the sign pattern of
+    each row of (J^T J)^-1 J^T); resolution_bound is the largest move of one
+    parameter on the ellipsoid dp^T J^T J dp = eps; a parameter at a bound gets 0."""
+    x = np.linspace(-5, 5, 201).astype(np.float32)
+    f, _ = A.model_and_jacobian("lorentzian", x, np.array([2.0, 0.3, 0.6]))
+    y = (f + 0.01 * np.random.default_rng(2).normal(size=x.size)).astype(np.float32)
+    ref = oracle.fit("port", "lorentzian", x, y[None], None, None, None, np.float64).params[0]
+    fr, J = A.model_and_jacobian("lorentzian", x, ref)
+    e = A.U32 * (np.abs(y.astype(np.float64)) + np.abs(fr))
+    G = np.linalg.solve(J.T @ J, J.T)
+    pb = A.perturbation_bound("lorentzian", x, y, ref)
+    for k in range(3):
+        dp = G @ (np.sign(G[k]) * e)  # the worst case for parameter k
+        assert abs(dp[k]) == pytest.approx(pb[k], rel=1e-12)
+        assert np.all(np.abs(G @ (np.random.default_rng(k).choice([-1.0, 1.0], x.size) * e)) <= pb * (1 + 1e-12))
+    rb = A.resolution_bound("lorentzian", x, y, ref)
+    eps = A.chi2_error_bound("lorentzian", x, y, ref)
+    inv = np.linalg.inv(J.T @ J)
+    for k in range(3):
+        dp = np.sqrt(eps / inv[k, k]) * inv[:, k]  # on the ellipsoid, extreme in k
+        assert dp @ (J.T @ J) @ dp == pytest.approx(eps, rel=1e-9)
+        assert dp[k] == pytest.approx(rb[k], rel=1e-9)
+    assert np.all(pb > 0) and np.all(rb > pb)  # sqrt(u32) against u32 scaling
+    at_bound = A.perturbation_bound("lorentzian", x, y, ref, lower=np.array([0.0, ref[1], 0.0]))
+    assert at_bound[1] == 0.0 and at_bound[0] > 0.0
+    s = A.summarize("lorentzian", x, y[None], ref[None], np.array([0]), np.array([1.0]), ref[None], np.array([0]),
+                    np.array([1.0]), x64=True, bounds=(np.full(3, -np.inf), np.full(3, np.inf)))
+    assert s["first_order_below_tol_fraction"] == 1.0 and s["within_tol_where_first_order_below_tol"] == 1.0
