@@ -21,8 +21,9 @@ namespace bf {
 // Guess kernel CTA shape per register-sort width V: up to 8 values per lane the
 // guess fits in 96 registers, so 128-thread CTAs, 5 per SM (20 warps); wider sorts
 // need 128 registers: 256 threads, 2 per SM.
+__host__ __device__ constexpr int guess_threads(int v) { return v > 0 && v <= 8 ? 128 : 256; }
 template <int V> struct GuessShapeCfg {
-    static constexpr int threads = V > 0 && V <= 8 ? 128 : 256;
+    static constexpr int threads = guess_threads(V);
     static constexpr int min_blocks = V > 0 && V <= 8 ? 5 : 2;
 };
 // LM kernel CTA shape per model.  The 3- and 4-parameter paired passes need 128
@@ -406,12 +407,20 @@ static cudaError_t launch_guess_typed(const float *x, const float *y, long long 
 struct GuessShape {
     int lanes, v;
 };
+// Every staged row takes shared memory, so from M=640 on the fits in flight per
+// SM are bounded by it: wider groups (up to 32 lanes) with at most 8 sort values a
+// lane keep 128-thread CTAs and split each fit over more lanes.  Measured on B200
+// (same results for every shape): pseudo-Voigt M=1024 8x16 1.18 ms -> 16x8 0.99 ms
+// per 262,144 fits; M=2048 16x16 1.26 ms -> 32x8 1.01 ms per 131,072 fits;
+// two-Lorentzian M=1024 7.78 -> 6.08 ms per 262,144 fits.
 __host__ __device__ inline GuessShape guess_shape(int m) {
     const int n1 = pow2_at_least(edge_count(m));
-    if (n1 <= 128)
+    if (n1 <= 64)
         return {8, n1 / 8 > 1 ? n1 / 8 : 1};
+    if (n1 <= 128)
+        return {16, 8};
     if (n1 <= 256)
-        return {16, 16};
+        return {32, 8};
     if (n1 <= 512)
         return {32, 16};
     return {32, 0};
@@ -444,8 +453,8 @@ static cudaError_t launch_guess_model(const float *x, const float *y, long long 
     case 802: return launch_guess_typed<MODEL, 8, 2>(x, y, n, m, guesses, status, sms, s, y_half);
     case 804: return launch_guess_typed<MODEL, 8, 4>(x, y, n, m, guesses, status, sms, s, y_half);
     case 808: return launch_guess_typed<MODEL, 8, 8>(x, y, n, m, guesses, status, sms, s, y_half);
-    case 816: return launch_guess_typed<MODEL, 8, 16>(x, y, n, m, guesses, status, sms, s, y_half);
-    case 1616: return launch_guess_typed<MODEL, 16, 16>(x, y, n, m, guesses, status, sms, s, y_half);
+    case 1608: return launch_guess_typed<MODEL, 16, 8>(x, y, n, m, guesses, status, sms, s, y_half);
+    case 3208: return launch_guess_typed<MODEL, 32, 8>(x, y, n, m, guesses, status, sms, s, y_half);
     case 3216: return launch_guess_typed<MODEL, 32, 16>(x, y, n, m, guesses, status, sms, s, y_half);
     default: return launch_guess_typed<MODEL, 32, 0>(x, y, n, m, guesses, status, sms, s, y_half);
     }
@@ -496,12 +505,8 @@ int group_smem_bytes(int model, int lanes, int m) {
 }
 
 static int guess_smem(int m) {
-    const GuessShape shape = guess_shape(m);
-    switch (shape.lanes) {
-    case 8: return guess_smem_bytes<8, 16>(m);
-    case 16: return guess_smem_bytes<16, 16>(m);
-    default: return shape.v ? guess_smem_bytes<32, 16>(m) : guess_smem_bytes<32, 0>(m);
-    }
+    const GuessShape s = guess_shape(m);
+    return 4 * (x_words(m) + (guess_threads(s.v) / s.lanes) * guess_group_words(m, s.lanes, s.v));
 }
 
 // Largest M with fits(M) (monotone) up to kMaxPoints.
