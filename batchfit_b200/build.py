@@ -52,8 +52,18 @@ def build(force: bool = False, verbose: bool = False, csrc: str = CSRC, lib: str
     os.makedirs(obj, exist_ok=True)
     cc = nvcc()
 
+    headers = [os.path.join(csrc, f) for f in HEADERS] + [os.path.join(ROOT, "include", "batchfit_cuda.h")]
+    # Objects are reused only when built with the same flags (recorded beside them).
+    stamp = os.path.join(obj, "flags.txt")
+    flags = " ".join([*ARCH, *FLAGS, *[f"-D{d}" for d in defines]])
+    same_flags = os.path.exists(stamp) and open(stamp).read() == flags
+    with open(stamp, "w") as fh:
+        fh.write(flags)
+
     def compile_one(src: str) -> str:
         target = os.path.join(obj, src.replace(".cu", ".o"))
+        if not force and same_flags and not _stale(target, [os.path.join(csrc, src), *headers]):
+            return target  # every header is shared: an object is current only if newer than all of them
         cmd = [cc, *ARCH, *FLAGS, *[f"-D{d}" for d in defines], "-c", os.path.join(csrc, src), "-o", target]
         if verbose:
             print(" ".join(cmd))

@@ -71,12 +71,15 @@ int choose_group_lanes(int model, uint32_t m, int requested) {
         // Points per lane between ~8 and ~128 keeps the group reduction and the FP64
         // control amortised without starving the scheduler of independent fits.  The
         // two-Lorentzian pass carries 8 parameters and 36 J^T J sums per point, so its
-        // groups widen sooner (measured on B200 at M=1024: 16 lanes run 1.4x faster
-        // than 8 and 5% faster than 32).
+        // groups widen sooner.  Measured on B200 (LM kernel, ~64M points per call):
+        // two-Lorentzian 16 lanes fastest from M=256 to 2048 (M=1024: 3.85 ms vs 5.19
+        // at 8, 4.76 at 32), 32 at 4096; the other models 8 lanes up to M=768, 16 at
+        // M=1024 (Lorentzian 0.364 vs 0.387 ms at 8) and 1536, 32 from M=2048
+        // (pseudo-Voigt 0.506 vs 0.513 at 16).
         if (model == 3)
             lanes = m <= 128 ? 8 : m <= 2048 ? 16 : 32;
         else
-            lanes = m <= 1024 ? 8 : m <= 2048 ? 16 : 32;
+            lanes = m < 1024 ? 8 : m < 2048 ? 16 : 32;
     }
     // Fewer, wider groups per CTA when the per-group spectrum buffers do not fit.
     while (lanes < 32 && bf::group_smem_bytes(model, lanes, int(m)) > kSmemLimit)
