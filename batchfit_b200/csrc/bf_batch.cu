@@ -87,6 +87,11 @@ struct BatchState {
     size_t host_bytes = 0;
     BatchArgs args{};
     cudaGraphExec_t graph = nullptr;
+    cudaGraph_t graph_src = nullptr;               // the captured graph: its nodes address `graph`'s
+    cudaGraphNode_t lm_nodes[kLmClassTypes] = {};  // LM kernel node per work-class type
+    uint32_t lm_enabled = kAllLmTypes;             // LM nodes enabled in `graph`
+    uint32_t kernels = 0;                          // kernels of the last direct launch
+    LmFork fork;                                   // side streams of the LM kernels
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bf_tuning tuning{};
     bool warmed = false; // kernels' attributes set (before any capture)
@@ -97,6 +102,9 @@ void release_batch_state(BatchState *st) {
         return;
     if (st->graph)
         cudaGraphExecDestroy(st->graph);
+    if (st->graph_src)
+        cudaGraphDestroy(st->graph_src);
+    release_lm_fork(st->fork);
     st->arena.release();
     if (st->host)
         cudaFreeHost(st->host);
@@ -126,6 +134,56 @@ int state_of(bf_cuda_context *ctx, BatchState **out) {
     return BF_OK;
 }
 
+void drop_graph(BatchState &st) {
+    if (st.graph)
+        cudaGraphExecDestroy(st.graph);
+    if (st.graph_src)
+        cudaGraphDestroy(st.graph_src);
+    st.graph = nullptr;
+    st.graph_src = nullptr;
+    std::fill(std::begin(st.lm_nodes), std::end(st.lm_nodes), nullptr);
+    st.lm_enabled = kAllLmTypes;
+}
+
+// Capture the pipeline (every LM kernel) on `stream` and instantiate it; keep the
+// captured graph and its LM kernel nodes, which batches enable per work-class type.
+cudaError_t capture_graph(BatchState &st, int sms, cudaStream_t stream) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        const cudaError_t le = launch_batch_pipeline(st.args, sms, stream, nullptr, nullptr, &st.fork);
+        e = cudaStreamEndCapture(stream, &g);
+        if (le != cudaSuccess)
+            e = le;
+    }
+    if (e == cudaSuccess)
+        e = cudaGraphInstantiate(&st.graph, g, 0);
+    if (e != cudaSuccess) {
+        if (g)
+            cudaGraphDestroy(g);
+        return e;
+    }
+    st.graph_src = g;
+    st.lm_enabled = kAllLmTypes;
+    size_t count = 0;
+    e = cudaGraphGetNodes(g, nullptr, &count);
+    std::vector<cudaGraphNode_t> nodes(count);
+    if (e == cudaSuccess && count)
+        e = cudaGraphGetNodes(g, nodes.data(), &count);
+    for (size_t i = 0; i < count && e == cudaSuccess; ++i) {
+        cudaGraphNodeType type;
+        e = cudaGraphNodeGetType(nodes[i], &type);
+        if (e != cudaSuccess || type != cudaGraphNodeTypeKernel)
+            continue;
+        cudaKernelNodeParams kp{};
+        e = cudaGraphKernelNodeGetParams(nodes[i], &kp);
+        for (int k = 0; k < kLmClassTypes && e == cudaSuccess; ++k)
+            if (kp.func == batch_lm_function(k))
+                st.lm_nodes[k] = nodes[i];
+    }
+    return e;
+}
+
 // Grow the arena (and drop the graph, whose arguments point into it).
 int reserve(BatchState &st, size_t segs, size_t items, size_t guess_floats) {
     if (segs <= st.seg_cap && items <= st.item_cap && guess_floats <= st.guess_cap && st.arena.ptr)
@@ -134,10 +192,7 @@ int reserve(BatchState &st, size_t segs, size_t items, size_t guess_floats) {
     const size_t i = std::max(items + items / 4, std::max<size_t>(st.item_cap, 1024));
     const size_t g = std::max(guess_floats + guess_floats / 4, std::max<size_t>(st.guess_cap, 4096));
     const Layout lay = layout_for(s, i, g);
-    if (st.graph) {
-        cudaGraphExecDestroy(st.graph);
-        st.graph = nullptr;
-    }
+    drop_graph(st);
     st.arena.release();
     cudaError_t e = st.arena.reserve(lay.total);
     if (e != cudaSuccess)
@@ -370,6 +425,14 @@ cudaError_t upload(BatchState &st, Plan &plan, cudaStream_t stream) {
 
 } // namespace
 
+// LM work-class types present in a plan (bit per type).
+uint32_t lm_types_of(const Plan &plan) {
+    uint32_t types = 0;
+    for (const WorkClass &c : plan.lm_classes)
+        types |= 1u << lm_class_type(c.model, c.lanes);
+    return types;
+}
+
 // Plan, upload and launch one batch on `stream` with the arena and graph of `st`
 // (events st.ev[0..3] bracket it).  Returns without waiting; *launched is false
 // when the batch had no fits.  One batch per state may be in flight: the pinned
@@ -390,28 +453,31 @@ int launch_planned(BatchState &st, const bf_batch_segment *segments, uint32_t co
     cudaError_t e = upload(st, plan, stream);
     if (e != cudaSuccess)
         return report_cuda(e, "batch descriptors");
-    const bool use_graph = (flags & BF_BATCH_NO_GRAPH) == 0 && st.warmed;
+    // Graph replay saves the host ~15 launches: it matters for short batches.  Large
+    // batches launch directly: measured on B200 (mixed stream, 65,536 fits), the
+    // LM kernels' three streams overlap their tails in direct launches (pipeline
+    // 4.38 ms) but not in the replayed graph (4.67 ms).
+    constexpr long long kGraphMaxItems = 32768;
+    const bool use_graph = (flags & BF_BATCH_NO_GRAPH) == 0 && st.warmed && plan.hdr.lm_items < kGraphMaxItems;
     e = cudaEventRecord(st.ev[0], stream);
+    const uint32_t types = lm_types_of(plan);
     if (e == cudaSuccess && use_graph) {
-        if (!st.graph) {
-            cudaGraph_t g = nullptr;
-            e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
-            if (e == cudaSuccess) {
-                const cudaError_t le = launch_batch_pipeline(st.args, sms, stream, nullptr, nullptr);
-                e = cudaStreamEndCapture(stream, &g);
-                if (le != cudaSuccess)
-                    e = le;
+        if (!st.graph)
+            e = capture_graph(st, sms, stream);
+        // Only the LM kernels of the batch's work-class types run.
+        for (int k = 0; k < kLmClassTypes && e == cudaSuccess; ++k) {
+            const bool want = (types >> k & 1u) != 0;
+            if (st.lm_nodes[k] && want != ((st.lm_enabled >> k & 1u) != 0)) {
+                e = cudaGraphNodeSetEnabled(st.graph, st.lm_nodes[k], want ? 1u : 0u);
+                st.lm_enabled ^= 1u << k;
             }
-            if (e == cudaSuccess)
-                e = cudaGraphInstantiate(&st.graph, g, 0);
-            if (g)
-                cudaGraphDestroy(g);
         }
         if (e == cudaSuccess)
             e = cudaGraphLaunch(st.graph, stream);
     } else if (e == cudaSuccess) {
-        e = launch_batch_pipeline(st.args, sms, stream, st.ev[1], st.ev[2]);
+        e = launch_batch_pipeline(st.args, sms, stream, st.ev[1], st.ev[2], &st.fork, types);
         st.warmed = st.warmed || e == cudaSuccess;
+        st.kernels = 3u + uint32_t(__builtin_popcount(types)); // prepare, guess, LM per type, covariance
     }
     if (e == cudaSuccess)
         e = cudaEventRecord(st.ev[3], stream);
@@ -434,7 +500,7 @@ int finish_planned(BatchState &st, bool graph_used, bf_cuda_timing *out) {
     bf_cuda_timing t{};
     t.kernel_ms = total;
     t.total_ms = total;
-    t.launches = graph_used ? 1u : 4u;
+    t.launches = graph_used ? 1u : st.kernels;
     t.batches = 1;
     if (!graph_used) {
         float g = 0.0f, l = 0.0f, c = 0.0f;
@@ -463,25 +529,14 @@ int prepare_planned(BatchState &st, size_t segs, size_t fits, int sms, cudaStrea
                                     static_cast<char *>(st.host) + st.lay.header, sizeof(empty),
                                     cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess)
-        e = launch_batch_pipeline(st.args, sms, stream, nullptr, nullptr);
+        e = launch_batch_pipeline(st.args, sms, stream, nullptr, nullptr, &st.fork);
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess)
         return report_cuda(e, "batch warm-up");
     st.warmed = true;
     if (!st.graph) {
-        cudaGraph_t g = nullptr;
-        e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) {
-            const cudaError_t le = launch_batch_pipeline(st.args, sms, stream, nullptr, nullptr);
-            e = cudaStreamEndCapture(stream, &g);
-            if (le != cudaSuccess)
-                e = le;
-        }
-        if (e == cudaSuccess)
-            e = cudaGraphInstantiate(&st.graph, g, 0);
-        if (g)
-            cudaGraphDestroy(g);
+        e = capture_graph(st, sms, stream);
         if (e != cudaSuccess)
             return report_cuda(e, "batch graph");
     }
@@ -497,6 +552,10 @@ bool planned_done(BatchState &st, cudaError_t *error) {
 int create_batch_state(BatchState **out) {
     auto *st = new BatchState();
     default_tuning(st->tuning);
+    if (const cudaError_t err = create_lm_fork(st->fork); err != cudaSuccess) {
+        release_batch_state(st);
+        return report_cuda(err, "batch streams");
+    }
     for (cudaEvent_t &e : st->ev) {
         const cudaError_t err = cudaEventCreate(&e);
         if (err != cudaSuccess) {

@@ -77,10 +77,30 @@ struct BatchArgs {
     unsigned long long *counters; // [kMaxClasses] LM classes, then [kMaxClasses] guess classes
 };
 
-// Host entry points (bf_batch_kernels.cu).  Every launch goes to `stream` with a
-// grid fixed by the device, so a captured sequence replays for any batch.
+// LM work-class types: one kernel each, index model * 3 + (8 -> 0, 16 -> 1, 32 -> 2).
+constexpr int kLmClassTypes = 12;
+constexpr uint32_t kAllLmTypes = (1u << kLmClassTypes) - 1u;
+inline int lm_class_type(int model, int lanes) { return model * 3 + (lanes == 8 ? 0 : lanes == 16 ? 1 : 2); }
+
+// Side streams for the LM kernels of a batch: the kernels of different work-class
+// types run on kLmStreams streams (the batch's own and these), so that one
+// kernel's tail fills with the next kernel's blocks.
+constexpr int kLmStreams = 3;
+struct LmFork {
+    cudaStream_t side[kLmStreams - 1] = {};
+    cudaEvent_t fork = nullptr, join[kLmStreams - 1] = {};
+};
+cudaError_t create_lm_fork(LmFork &f);
+void release_lm_fork(LmFork &f);
+
+// Host entry points (bf_batch_kernels.cu).  Every launch goes to `stream` (and
+// the fork's side streams) with a grid fixed by the device, so a captured sequence
+// replays for any batch.  The LM kernels of the types in `lm_types` (bit per type)
+// are launched; a captured pipeline holds all of them.
 cudaError_t launch_batch_pipeline(const BatchArgs &b, int sms, cudaStream_t stream, cudaEvent_t guessed,
-                                  cudaEvent_t fitted);
+                                  cudaEvent_t fitted, const LmFork *fork, uint32_t lm_types = kAllLmTypes);
+// The LM kernel of a work-class type (to find its node in a captured graph).
+const void *batch_lm_function(int type);
 // Guess code path (lanes, register width) for M; false when M/10 exceeds the
 // sorting buffer.
 bool batch_guess_shape(int m, int *lanes, int *v);

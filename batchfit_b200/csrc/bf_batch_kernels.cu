@@ -102,26 +102,20 @@ __device__ __forceinline__ void lm_class(const BatchArgs &b, const WorkClass &cl
     }
 }
 
-__global__ void __launch_bounds__(kBatchLmBlock, kBatchLmMinBlocks) batch_lm_kernel(BatchArgs b) {
+// One LM kernel per work-class type (model, lanes per fit), each walking only its
+// own classes: a kernel holding several instantiations spills (1.5-2.2 KB of
+// stack), one holding a single instantiation keeps lm_kernel's registers.
+template <int MODEL, int G>
+__global__ void __launch_bounds__(kBatchLmBlock, MODEL == kTwoLorentzian ? 3 : 4) batch_lm_kernel(BatchArgs b) {
     extern __shared__ __align__(16) double lm_smem[];
     double *warp_state = lm_smem + (threadIdx.x / 32) * kLmWarpDoubles;
     const int classes = b.hdr->lm_classes;
+    const int group = int(threadIdx.x & 31u) / G;
+    double *state = warp_state + group * kLmSlotDoubles;
     for (int c = 0; c < classes; ++c) {
         const WorkClass cls = b.lm_classes[c];
-        const int group = int(threadIdx.x & 31u) / cls.lanes;
-        double *state = warp_state + group * kLmSlotDoubles;
-        switch (cls.model * 100 + cls.lanes) {
-#define BF_LM_CASE(MODEL, G)                                                                                   \
-    case MODEL * 100 + G: lm_class<MODEL, G>(b, cls, b.counters + c, state); break;
-#define BF_LM_MODEL(MODEL) BF_LM_CASE(MODEL, 8) BF_LM_CASE(MODEL, 16) BF_LM_CASE(MODEL, 32)
-            BF_LM_MODEL(0)
-            BF_LM_MODEL(1)
-            BF_LM_MODEL(2)
-            BF_LM_MODEL(3)
-#undef BF_LM_MODEL
-#undef BF_LM_CASE
-        default: break;
-        }
+        if (cls.model == MODEL && cls.lanes == G)
+            lm_class<MODEL, G>(b, cls, b.counters + c, state);
         __syncwarp();
     }
 }
@@ -200,8 +194,13 @@ __global__ void __launch_bounds__(256) synthetic_kernel(int m, long long n, unsi
 
 struct Grids {
     int device = -1;
-    int guess = 0, lm = 0;
+    int guess = 0, lm[kLmClassTypes] = {}; // LM grid per work-class type
 };
+
+using LmKernel = void (*)(BatchArgs);
+#define BF_LM_FN(MODEL) batch_lm_kernel<MODEL, 8>, batch_lm_kernel<MODEL, 16>, batch_lm_kernel<MODEL, 32>
+constexpr LmKernel kLmKernels[kLmClassTypes] = {BF_LM_FN(0), BF_LM_FN(1), BF_LM_FN(2), BF_LM_FN(3)};
+#undef BF_LM_FN
 
 // Grids per device, resolved once (outside any stream capture: the first batch
 // on a context launches directly).
@@ -220,18 +219,20 @@ cudaError_t grids_for(int sms, Grids &out) {
         out = cache[device];
         return cudaSuccess;
     }
-    int per_sm_guess = 0, per_sm_lm = 0;
+    int per_sm_guess = 0;
     e = batch_guess_blocks_per_sm(&per_sm_guess);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(batch_lm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kLmSmem);
-    if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_lm, batch_lm_kernel, kBatchLmBlock, kLmSmem);
+    Grids g;
+    for (int k = 0; k < kLmClassTypes && e == cudaSuccess; ++k) {
+        int per_sm = 0;
+        e = cudaFuncSetAttribute(kLmKernels[k], cudaFuncAttributeMaxDynamicSharedMemorySize, kLmSmem);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kLmKernels[k], kBatchLmBlock, kLmSmem);
+        g.lm[k] = sms * (per_sm > 0 ? per_sm : 1);
+    }
     if (e != cudaSuccess)
         return e;
-    Grids g;
     g.device = device;
     g.guess = sms * (per_sm_guess > 0 ? per_sm_guess : 1);
-    g.lm = sms * (per_sm_lm > 0 ? per_sm_lm : 1);
     cache[device] = g;
     out = g;
     return cudaSuccess;
@@ -273,8 +274,38 @@ cudaError_t launch_synthetic(int model, int m, long long n, unsigned seed, float
     return cudaGetLastError();
 }
 
+const void *batch_lm_function(int type) {
+    return type >= 0 && type < kLmClassTypes ? reinterpret_cast<const void *>(kLmKernels[type]) : nullptr;
+}
+
+cudaError_t create_lm_fork(LmFork &f) {
+    cudaError_t e = cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming);
+    for (int s = 0; s < kLmStreams - 1 && e == cudaSuccess; ++s) {
+        e = cudaStreamCreateWithFlags(&f.side[s], cudaStreamNonBlocking);
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&f.join[s], cudaEventDisableTiming);
+    }
+    return e;
+}
+
+void release_lm_fork(LmFork &f) {
+    for (int s = 0; s < kLmStreams - 1; ++s) {
+        if (f.side[s]) {
+            cudaStreamSynchronize(f.side[s]);
+            cudaStreamDestroy(f.side[s]);
+        }
+        if (f.join[s])
+            cudaEventDestroy(f.join[s]);
+        f.side[s] = nullptr;
+        f.join[s] = nullptr;
+    }
+    if (f.fork)
+        cudaEventDestroy(f.fork);
+    f.fork = nullptr;
+}
+
 cudaError_t launch_batch_pipeline(const BatchArgs &b, int sms, cudaStream_t stream, cudaEvent_t guessed,
-                                  cudaEvent_t fitted) {
+                                  cudaEvent_t fitted, const LmFork *fork, uint32_t lm_types) {
     Grids grids;
     cudaError_t e = grids_for(sms, grids);
     if (e != cudaSuccess)
@@ -286,7 +317,30 @@ cudaError_t launch_batch_pipeline(const BatchArgs &b, int sms, cudaStream_t stre
     launch_batch_guess(b, grids.guess, stream);
     if (guessed && (e = cudaEventRecord(guessed, stream)) != cudaSuccess)
         return e;
-    batch_lm_kernel<<<grids.lm, kBatchLmBlock, kLmSmem, stream>>>(b);
+    // Heaviest types first (two-Lorentzian, then pseudo-Voigt, ...), dealt round-robin
+    // over the streams.
+    cudaStream_t lanes[kLmStreams] = {stream};
+    const int streams = fork ? kLmStreams : 1;
+    if (fork) {
+        e = cudaEventRecord(fork->fork, stream);
+        for (int s = 1; s < kLmStreams && e == cudaSuccess; ++s) {
+            lanes[s] = fork->side[s - 1];
+            e = cudaStreamWaitEvent(lanes[s], fork->fork, 0);
+        }
+        if (e != cudaSuccess)
+            return e;
+    }
+    int dealt = 0;
+    for (int k = kLmClassTypes - 1; k >= 0; --k)
+        if (lm_types >> k & 1u)
+            kLmKernels[k]<<<grids.lm[k], kBatchLmBlock, kLmSmem, lanes[dealt++ % streams]>>>(b);
+    for (int s = 1; s < streams && e == cudaSuccess; ++s) {
+        e = cudaEventRecord(fork->join[s - 1], lanes[s]);
+        if (e == cudaSuccess)
+            e = cudaStreamWaitEvent(stream, fork->join[s - 1], 0);
+    }
+    if (e != cudaSuccess)
+        return e;
     if (fitted && (e = cudaEventRecord(fitted, stream)) != cudaSuccess)
         return e;
     batch_covariance_kernel<<<sms * 8, 128, 0, stream>>>(b);

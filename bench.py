@@ -341,7 +341,7 @@ def mixed_section(ctx, dev):
                     f"{len(segs)} requests (one per model and M, sharing x)",
         "batched": {"fits_per_s": n_fits / (tuned_dev * 1e-3), "device_ms": round(tuned_dev, 3),
                     "call_ms": round(tuned_wall, 3), "kernels_no_graph": split,
-                    "what": "autotuned lanes, one persistent launch per kernel, graph replay"},
+                    "what": "autotuned lanes; persistent guess and covariance launches, one LM launch per (model, lanes) class type over three streams; direct launches (graph replay below 32,768 fits)"},
         "fixed_mapping": {"fits_per_s": n_fits / (fixed_dev * 1e-3), "device_ms": round(fixed_dev, 3),
                           "call_ms": round(fixed_wall, 3), "what": "one launch, every fit on one warp, request order"},
         "plain_per_request": {"fits_per_s": n_fits / (plain_dev * 1e-3), "device_ms": round(plain_dev, 3),
