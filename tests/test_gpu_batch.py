@@ -125,6 +125,31 @@ def test_graph_replay_and_arena_growth(bf):
             np.testing.assert_array_equal(a[k], b[k])
 
 
+def test_graph_enables_only_the_batch_class_types(bf):
+    """The replayed graph holds one LM kernel per (model, lanes) class type and a
+    batch enables only its own types: batches whose type sets change from call to
+    call (one model, another, all, a subset) equal their direct launches bit for
+    bit, and so does a batch past the graph's size (launched directly)."""
+    reqs = requests(seed=80)
+    by_model = {m: [r for r in reqs if r["model"] == m] for m in P}
+    sequence = [by_model["gaussian"], by_model["two_lorentzian"], reqs, by_model["pseudo_voigt"],
+                by_model["lorentzian"] + by_model["two_lorentzian"], by_model["gaussian"]]
+    for batch in sequence:
+        direct = [to_np(r) for r in bf.fit_batch(batch, graph=False)]
+        replayed = [to_np(r) for r in bf.fit_batch(batch)]
+        for a, b in zip(direct, replayed):
+            for k in a:
+                np.testing.assert_array_equal(a[k], b[k])
+    x, y, bounds = spectra("pseudo_voigt", 40000, 64, 81)
+    big = [dict(x=x, y=y, model="pseudo_voigt", bounds=bounds)] + by_model["two_lorentzian"]
+    got = [to_np(r) for r in bf.fit_batch(big)]
+    ref = [to_np(r) for r in bf.fit_batch(big, graph=False)]
+    for a, b in zip(got, ref):
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k])
+    assert np.isin(got[0]["status"], (0, 5)).mean() > 0.9
+
+
 def test_fixed_mapping_is_one_warp_per_fit(bf):
     reqs = requests(seed=90)
     fixed = bf.fit_batch(reqs, fixed_mapping=True)
