@@ -192,56 +192,13 @@ template <int MODEL, bool PRE = false> struct Signal {
     }
 };
 
-// Visit every interior sample j (1 <= j <= m-2) in order, G at a time, with its
-// smoothed value and both smoothed neighbours: each smoothed sample is computed
-// once and its neighbours come from the adjacent lanes (the first lane's left
-// neighbour is carried from the previous chunk; the last lane computes its right
-// neighbour).  Two chunks are in flight per step.  f(j, value, left, right) runs on
-// lanes with an interior j.  Returns whether every signal sample is finite.
-template <int G, class S, class F>
-__device__ __forceinline__ bool scan_smoothed(const Group<G> &g, const S &s, F &&f) {
-    const int m = s.m;
-    const float first = s.at(0);
-    float carry = first; // smooth(0) is the raw edge sample
-    bool finite = isfinite(first) & isfinite(s.at(m - 1));
-    for (int t0 = 1; t0 + 1 < m; t0 += 2 * G) {
-        const int j0 = t0 + int(g.lane), j1 = j0 + G;
-        const bool in0 = j0 + 1 < m, in1 = j1 + 1 < m;
-        const float s0 = in0 ? s.at(j0) : 0.0f, s1 = in1 ? s.at(j1) : 0.0f;
-        finite = finite & isfinite(s0) & isfinite(s1);
-        const float v0 = in0 ? radd(radd(rmul(0.25f, s.at(j0 - 1)), rmul(0.5f, s0)), rmul(0.25f, s.at(j0 + 1)))
-                             : 0.0f;
-        const float v1 = in1 ? radd(radd(rmul(0.25f, s.at(j1 - 1)), rmul(0.5f, s1)), rmul(0.25f, s.at(j1 + 1)))
-                             : 0.0f;
-        float l0 = g.prev(v0), l1 = g.prev(v1);
-        float r0 = g.next(v0), r1 = g.next(v1);
-        const float last0 = g.bcast(v0, G - 1), first1 = g.bcast(v1, 0), last1 = g.bcast(v1, G - 1);
-        if (g.lane == 0) {
-            l0 = carry;
-            l1 = last0;
-        }
-        if (g.lane == G - 1)
-            r0 = first1;
-        if (in0 && j0 + 2 >= m)
-            r0 = s.smooth(j0 + 1);
-        if (in1 && (g.lane == G - 1 || j1 + 2 >= m))
-            r1 = s.smooth(j1 + 1);
-        carry = last1;
-        if (in0)
-            f(j0, v0, l0, r0);
-        if (in1)
-            f(j1, v1, l1, r1);
-    }
-    return finite;
-}
-
 // ------------------------------------------------------- chunked sweep --
-// The same sweep over a staged row in 4-sample chunks.  Chunk c (samples 4c..4c+3)
+// The tallest-smoothed-maximum sweep in 4-sample chunks.  Chunk c (samples 4c..4c+3)
 // goes to group lane c mod G at step c / G; that lane also reads chunk c-1 and
 // tests samples 4c-2..4c+1, whose smoothed values and smoothed neighbours need
-// samples 4c-4..4c+3 only: two 16-byte reads a step, no shuffles.  Chunks
-// 0..m/4 cover every interior sample.  The row must be 16-byte aligned with
-// round_up(m, 4) floats.
+// samples 4c-4..4c+3 only: no shuffles, and from a staged row (16-byte aligned,
+// round_up(m, 4) floats) two 16-byte reads a step.  Chunks 0..m/4 cover every
+// interior sample.
 __host__ __device__ inline int chunk_steps(int m, int lanes) { return (m / 4 + lanes) / lanes; }
 // Candidate-bit words per lane: 4 bits a step.
 __host__ __device__ inline int chunk_words(int m, int lanes) { return (chunk_steps(m, lanes) + 7) / 8; }
@@ -255,14 +212,26 @@ __device__ __forceinline__ int chunk_sample(int lane, int b, int lanes) {
 // initial_guess.hpp:173-174), else 0 (a value that never beats a height >= 0).
 // `fin` accumulates whether the chunk's own samples are finite.  EDGE: the step
 // may touch sample 0, sample m-1 or samples past the row (masked, unsmoothed ends).
-template <bool EDGE, bool SUB>
-__device__ __forceinline__ void chunk_step(const float4 *row, int m, float level, int c, float (&cv)[4], bool &fin) {
-    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+// VEC: the row is staged (16-byte aligned, padded to round_up(m, 4)) and read 16
+// bytes at a time, as y (SUB: the signal is y - level) or as the signal itself;
+// otherwise the samples come one by one from the Signal `sig` (any alignment, no
+// padding: samples outside the row are not read).
+template <bool EDGE, bool SUB, bool VEC, class S>
+__device__ __forceinline__ void chunk_step(const float4 *row, const S &sig, int m, float level, int c,
+                                           float (&cv)[4], bool &fin) {
     const int j0 = 4 * c - 4;
-    const float4 a = !EDGE || (c >= 1 && j0 < m) ? row[c - 1] : zero;
-    const float4 b = !EDGE || j0 + 4 < m ? row[c] : zero;
-    float s[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}; // samples 4c-4+i
-    if constexpr (SUB) {
+    float s[8]; // samples 4c-4+i
+    if constexpr (VEC) {
+        const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float4 a = !EDGE || (c >= 1 && j0 < m) ? row[c - 1] : zero;
+        const float4 b = !EDGE || j0 + 4 < m ? row[c] : zero;
+        s[0] = a.x, s[1] = a.y, s[2] = a.z, s[3] = a.w, s[4] = b.x, s[5] = b.y, s[6] = b.z, s[7] = b.w;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            s[i] = !EDGE || (j0 + i >= 0 && j0 + i < m) ? sig.at(j0 + i) : 0.0f;
+    }
+    if constexpr (VEC && SUB) {
         // The signal of a baseline-only model, y - level (Signal::raw), two at a time.
 #pragma unroll
         for (int i = 0; i < 8; i += 2) {
@@ -310,8 +279,8 @@ __device__ __forceinline__ void chunk_step(const float4 *row, int m, float level
 // (positive smoothed local maxima, bit 4k+t for sample 4(lane+kG)-2+t, words at
 // bits[w*G]).  SUB: the row holds y and the signal is y - level.  Returns whether
 // the lane's signal samples are finite.
-template <int G, bool BITS, bool SUB>
-__device__ __forceinline__ bool chunk_sweep(const Group<G> &g, const float *signal, int m, float level,
+template <int G, bool BITS, bool SUB, bool VEC, class S>
+__device__ __forceinline__ bool chunk_sweep(const Group<G> &g, const S &sig, const float *signal, int m, float level,
                                             float &height, int &first, unsigned *bits) {
     const float4 *row = reinterpret_cast<const float4 *>(signal);
     const int steps = chunk_steps(m, G);
@@ -321,7 +290,7 @@ __device__ __forceinline__ bool chunk_sweep(const Group<G> &g, const float *sign
     unsigned word = 0;
     auto visit = [&](auto edge, int k) {
         float cv[4];
-        chunk_step<decltype(edge)::value, SUB>(row, m, level, int(g.lane) + k * G, cv, fin);
+        chunk_step<decltype(edge)::value, SUB, VEC>(row, sig, m, level, int(g.lane) + k * G, cv, fin);
         const float top = fmaxf(fmaxf(cv[0], cv[1]), fmaxf(cv[2], cv[3]));
         if (top > height) {
             height = top;
@@ -353,7 +322,7 @@ __device__ __forceinline__ bool chunk_sweep(const Group<G> &g, const float *sign
         const int c = int(g.lane) + best * G;
         float cv[4];
         bool unused = true;
-        chunk_step<true, SUB>(row, m, level, c, cv, unused);
+        chunk_step<true, SUB, VEC>(row, sig, m, level, c, cv, unused);
 #pragma unroll
         for (int t = 3; t >= 0; --t)
             if (cv[t] == height)
@@ -485,16 +454,10 @@ __device__ PeakFeature find_peak(const Group<G> &g, const S &s, const float *xs,
 // takes blocks l, l+G, ...
 constexpr int kWalkBlock = 32;
 __host__ __device__ inline int walk_blocks(int m) { return (m + kWalkBlock - 1) / kWalkBlock; }
-// Interior samples j = 1 + lane + k*G (j <= m - 2) of one group lane.
-__host__ __device__ inline int lane_samples(int m, int lane, int lanes) {
-    return m - 3 - lane >= 0 ? (m - 3 - lane) / lanes + 1 : 0;
-}
-// Scratch words of the second-peak search: four block arrays, then one candidate
-// bit per interior sample (lane-wise words, word-major).
-// (Either sweep's layout: the lane-interleaved or the chunked one.)
+// Scratch words of the second-peak search: four block arrays, then the chunked
+// sweep's candidate bits (4 per step and lane; lane-wise words, word-major).
 __host__ __device__ inline int second_peak_words(int m, int lanes) {
-    const int interleaved = (lane_samples(m, 0, lanes) + 31) / 32, chunked = chunk_words(m, lanes);
-    return 4 * walk_blocks(m) + lanes * (interleaved > chunked ? interleaved : chunked);
+    return 4 * walk_blocks(m) + lanes * chunk_words(m, lanes);
 }
 template <int G, class S>
 __device__ void block_extrema(const Group<G> &g, const S &s, float *bmin, float *bmax) {
@@ -712,33 +675,14 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
     // checks that every signal sample is finite (initial_guess.hpp:158-162); both
     // failures end in invalid_input, so their order does not matter.  For the
     // two-Lorentzian it also records every positive smoothed local maximum, the
-    // candidates of the second-peak search, as one bit per sample of the lane
-    // (lane l visits j = 1 + l + k*G: bit k of word k/32, words stored
-    // word-major after the block extrema in `scratch`).
+    // candidates of the second-peak search, as bits of the lane (bit 4k+t of
+    // lane l is sample 4(l + kG) - 2 + t; words stored word-major after the block
+    // extrema in `scratch`).
     float height = 0.0f;
     int first = m;
     [[maybe_unused]] unsigned *cand_bits = reinterpret_cast<unsigned *>(scratch + 4 * walk_blocks(m));
-    bool signal_finite;
-    if constexpr (PRE) {
-        signal_finite = chunk_sweep<G, paired, !overwrite>(g, ys, m, level, height, first, cand_bits);
-    } else {
-        [[maybe_unused]] unsigned word = 0;
-        signal_finite = scan_smoothed<G>(g, s, [&](int j, float v, float left, float right) {
-            const bool peak = v > 0.0f && v > left && v >= right;
-            if (peak && v > height) {
-                height = v;
-                first = j;
-            }
-            if constexpr (paired) {
-                const int k = int(unsigned(j - 1 - int(g.lane)) / G);
-                word |= unsigned(peak) << (k & 31);
-                if ((k & 31) == 31 || j + G + 1 >= m) {
-                    cand_bits[(k >> 5) * G + int(g.lane)] = word;
-                    word = 0;
-                }
-            }
-        });
-    }
+    const bool signal_finite =
+        chunk_sweep<G, paired, !overwrite, PRE>(g, s, ys, m, level, height, first, cand_bits);
     if (!g.all(signal_finite))
         return kGuessInvalid;
     argmax_pair(g, height, first);
@@ -783,9 +727,8 @@ __device__ int initial_guess(const Group<G> &g, const XConst &xc, const float *x
             const int bins = idx > first ? idx - first : first - idx;
             return !(bins < 3 || fabsf(rsub(xs[idx], primary.center)) < separation);
         };
-        const int words = PRE ? chunk_words(m, G) : (lane_samples(m, int(g.lane), G) + 31) >> 5;
-        // Sample of bit b of this lane's candidate words (the layout of the sweep used).
-        auto cand_sample = [&](int b) { return PRE ? chunk_sample(int(g.lane), b, G) : 1 + int(g.lane) + b * G; };
+        const int words = chunk_words(m, G);
+        auto cand_sample = [&](int b) { return chunk_sample(int(g.lane), b, G); };
         const unsigned *bits = cand_bits + int(g.lane);
         int second = m;
         float v1 = 0.0f, v2 = 0.0f;
