@@ -26,15 +26,18 @@ template <int V> struct GuessShapeCfg {
     static constexpr int threads = guess_threads(V);
     static constexpr int min_blocks = V > 0 && V <= 8 ? 5 : 2;
 };
-// LM kernel CTA shape per model.  The 3- and 4-parameter paired passes need 128
-// registers a thread: 128-thread CTAs, 4 per SM (16 warps; at 5 per SM, 96
-// registers, they spill and run 7% slower on B200).  The two-Lorentzian
-// state (8 parameters, 36 J^T J sums, an 8x8 FP64 Cholesky) spills heavily at 128
-// registers; 128-thread CTAs, 3 per SM, allow 168 (12 warps per SM, little
-// spilling) -- measured 5% faster on B200 than 256 threads, 2 per SM.
-template <int MODEL> struct LmShape {
+// LM kernel CTA shape per model and group width.  The 3- and 4-parameter paired
+// passes need 128 registers a thread: 128-thread CTAs, 4 per SM (16 warps).  At 5
+// per SM (96 registers) the pseudo-Voigt spills 82 bytes and runs 5-20% slower, but
+// the Lorentzian and Gaussian at 8 lanes fit (95-96 registers, 0-4 bytes) and run
+// 2-7% faster at M = 256 and 512, where the lane rule uses 8 lanes.  The
+// two-Lorentzian state (8 parameters, 36 J^T J sums, an 8x8 FP64 Cholesky) spills
+// heavily at 128 registers; 128-thread CTAs, 3 per SM, allow 168 (12 warps per SM,
+// little spilling) -- measured 5% faster on B200 than 256 threads, 2 per SM.
+template <int MODEL, int G = 8> struct LmShape {
     static constexpr int threads = 128;
-    static constexpr int min_blocks = MODEL == kTwoLorentzian ? 3 : 4;
+    static constexpr int min_blocks =
+        MODEL == kTwoLorentzian ? 3 : (MODEL != kPseudoVoigt && G == 8) ? 5 : 4;
 };
 
 // Per-group shared memory, in 4-byte words, padded so that consecutive groups of a
@@ -150,7 +153,7 @@ __global__ void __launch_bounds__(GuessShapeCfg<V>::threads, GuessShapeCfg<V>::m
 
 // --------------------------------------------------------------- LM kernel --
 template <int MODEL, int G>
-__global__ void __launch_bounds__(LmShape<MODEL>::threads, LmShape<MODEL>::min_blocks) lm_kernel(FitArgs a) {
+__global__ void __launch_bounds__(LmShape<MODEL, G>::threads, LmShape<MODEL, G>::min_blocks) lm_kernel(FitArgs a) {
     constexpr int P = Model<MODEL>::P;
     constexpr int kGroups = LmShape<MODEL>::threads / G;
     extern __shared__ __align__(16) float smem[];
