@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) synthetic_kernel(int m, long long n, unsi
 
 struct Grids {
     int device = -1;
-    int guess = 0, lm[kLmClassTypes] = {}; // LM grid per work-class type
+    int guess = 0, lm[kLmClassTypes] = {}; // guess grid, LM grid per work-class type
 };
 
 using LmKernel = void (*)(BatchArgs);
@@ -202,8 +202,8 @@ using LmKernel = void (*)(BatchArgs);
 constexpr LmKernel kLmKernels[kLmClassTypes] = {BF_LM_FN(0), BF_LM_FN(1), BF_LM_FN(2), BF_LM_FN(3)};
 #undef BF_LM_FN
 
-// Grids per device, resolved once (outside any stream capture: the first batch
-// on a context launches directly).
+// Grids for `sms` SMs' worth of blocks: blocks per SM resolved once per device
+// (outside any stream capture: the first batch on a context launches directly).
 cudaError_t grids_for(int sms, Grids &out) {
     constexpr int kDevices = 64;
     static Grids cache[kDevices];
@@ -215,8 +215,14 @@ cudaError_t grids_for(int sms, Grids &out) {
     if (device < 0 || device >= kDevices)
         return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(mutex);
+    auto scaled = [&](const Grids &per_sm) {
+        out = per_sm;
+        out.guess *= sms;
+        for (int &l : out.lm)
+            l *= sms;
+    };
     if (cache[device].device == device) {
-        out = cache[device];
+        scaled(cache[device]);
         return cudaSuccess;
     }
     int per_sm_guess = 0;
@@ -227,14 +233,14 @@ cudaError_t grids_for(int sms, Grids &out) {
         e = cudaFuncSetAttribute(kLmKernels[k], cudaFuncAttributeMaxDynamicSharedMemorySize, kLmSmem);
         if (e == cudaSuccess)
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kLmKernels[k], kBatchLmBlock, kLmSmem);
-        g.lm[k] = sms * (per_sm > 0 ? per_sm : 1);
+        g.lm[k] = per_sm > 0 ? per_sm : 1;
     }
     if (e != cudaSuccess)
         return e;
     g.device = device;
-    g.guess = sms * (per_sm_guess > 0 ? per_sm_guess : 1);
-    cache[device] = g;
-    out = g;
+    g.guess = per_sm_guess > 0 ? per_sm_guess : 1;
+    cache[device] = g; // blocks per SM
+    scaled(g);
     return cudaSuccess;
 }
 

@@ -89,6 +89,7 @@ struct Slot {
     cudaEvent_t done = nullptr; // after the batch, the copies back and the frees
     std::vector<std::shared_ptr<Request>> requests;
     bool busy = false, graph_used = false, launched = false;
+    bool large = false; // runs a request predicted to take longer than kBatchTargetMs
 };
 
 } // namespace
@@ -233,8 +234,11 @@ bool admit(bf_server *s) {
     return true;
 }
 
-// Launch the ready requests (up to max_batch_fits) on a free slot.
-bool launch(bf_server *s, Slot &slot) {
+// Launch the ready requests (up to max_batch_fits) on a free slot.  Without
+// allow_large, requests predicted to take longer than kBatchTargetMs stay queued:
+// at most one slot runs a large request, so the other one is always free for
+// short batches within a short batch's time.
+bool launch(bf_server *s, Slot &slot, bool allow_large) {
     // Copies complete in admission order, so the requests whose inputs are on the
     // device are a prefix of the ready list: a batch never waits for other
     // requests' copies.
@@ -260,6 +264,8 @@ bool launch(bf_server *s, Slot &slot) {
         }
         if (!take.empty() && s->opt.max_batch_fits && fits + n > s->opt.max_batch_fits)
             break;
+        if (!allow_large && t > kBatchTargetMs)
+            continue; // waits for the other slot's large request to finish
         if (!take.empty() && predicted + t > kBatchTargetMs) {
             if (t > kBatchTargetMs)
                 continue; // large: its own batch, later
@@ -285,8 +291,17 @@ bool launch(bf_server *s, Slot &slot) {
         segs.push_back(r->seg);
     cudaError_t e = cudaSuccess;
     bool launched = false;
-    const int rc = bf::host::launch_planned(*slot.state, segs.data(), uint32_t(segs.size()), s->opt.batch_flags,
-                                            s->sms, slot.stream, &launched, &slot.graph_used);
+    // A large batch's persistent kernels would hold every SM until its work drains,
+    // and a short batch on the other slot could not start before.  With two slots a
+    // large batch launches directly with grids for three quarters of the SMs' blocks,
+    // which the hardware spreads over all SMs: every SM keeps room for the other
+    // slot's blocks.
+    const bool large = predicted > kBatchTargetMs;
+    const bool shared = large && s->opt.max_in_flight != 1;
+    const int rc = bf::host::launch_planned(*slot.state, segs.data(), uint32_t(segs.size()),
+                                            s->opt.batch_flags | (shared ? BF_BATCH_NO_GRAPH : 0u),
+                                            shared ? s->sms * 3 / 4 : s->sms, slot.stream, &launched,
+                                            &slot.graph_used);
     slot.launched = launched;
     if (rc != BF_OK) {
         // The batch could not be formed (a request failed validation on the device
@@ -303,6 +318,7 @@ bool launch(bf_server *s, Slot &slot) {
         report_cuda(e, "server launch");
         return false;
     }
+    slot.large = large;
     slot.requests = std::move(take);
     slot.busy = true;
     std::lock_guard<std::mutex> lock(s->mutex);
@@ -414,8 +430,12 @@ void scheduler(bf_server *s) {
         if (ok)
             ok = admit(s);
         for (int i = 0; i < slots && ok && !s->ready.empty(); ++i)
-            if (!s->slot[i].busy)
-                ok = launch(s, s->slot[i]);
+            if (!s->slot[i].busy) {
+                // With two slots, a large request may take a slot only while the
+                // other one is not running one.
+                const bool other_large = slots == 2 && s->slot[1 - i].busy && s->slot[1 - i].large;
+                ok = launch(s, s->slot[i], !other_large);
+            }
         if (!ok) {
             fail_everything(s, bf_cuda_last_error());
             return;

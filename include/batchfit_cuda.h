@@ -222,7 +222,9 @@ int bf_cuda_set_tuning(bf_cuda_context *ctx, const bf_tuning *in);
  * form the next one, which starts as soon as they are copied in and overlaps the
  * running batch's tail.  A batch grows to about 1 ms of predicted device time; a
  * request predicted to take longer runs in a batch of its own, and smaller requests
- * that arrive after it may start before it.  Outputs are copied into the request's host buffers, which
+ * that arrive after it may start before it.  At most one slot runs such a large
+ * batch, launched with kernels sized for three quarters of the GPU's blocks, so
+ * that short batches on the other slot always find room on every SM.  Outputs are copied into the request's host buffers, which
  * stay owned by the caller and must stay valid until the request completes.  A
  * request's result is the one bf_cuda_fit_batch gives for it; batch-mates only
  * change its lanes per fit (so results agree within the parity tolerances). */
