@@ -190,7 +190,10 @@ typedef struct bf_batch_segment {
 #define BF_BATCH_FIXED_MAPPING 1u /* the plain mapping: one fit per warp (32 lanes), segments in call order */
 #define BF_BATCH_NO_GRAPH 2u      /* launch the kernels one by one (per-kernel timing) instead of a graph replay */
 
-/* Synchronous: returns when every segment's outputs are written. */
+/* Synchronous: returns when every segment's outputs are written.  Batches under
+ * 32,768 fits replay a CUDA graph captured on the context (the LM kernels of the
+ * batch's own (model, lanes) types enabled); larger ones launch their kernels
+ * directly.  Either way the results are the same. */
 int bf_cuda_fit_batch(bf_cuda_context *ctx, const bf_batch_segment *segments, uint32_t count, uint32_t flags);
 uint32_t bf_cuda_batch_max_points(void);
 
@@ -224,8 +227,9 @@ int bf_cuda_set_tuning(bf_cuda_context *ctx, const bf_tuning *in);
  * request predicted to take longer runs in a batch of its own, and smaller requests
  * that arrive after it may start before it.  At most one slot runs such a large
  * batch, launched with kernels sized for three quarters of the GPU's blocks, so
- * that short batches on the other slot always find room on every SM.  Outputs are copied into the request's host buffers, which
- * stay owned by the caller and must stay valid until the request completes.  A
+ * that short batches on the other slot always find room on every SM.  Outputs are
+ * copied into the request's host buffers, which stay owned by the caller and must
+ * stay valid until the request completes.  A
  * request's result is the one bf_cuda_fit_batch gives for it; batch-mates only
  * change its lanes per fit (so results agree within the parity tolerances). */
 typedef struct bf_server bf_server;
