@@ -412,6 +412,39 @@ int prepare_segment(const bf_fit_args *args, const bf_fit_outputs *out, uint32_t
     return BF_OK;
 }
 int default_lanes(int model, uint32_t m) { return choose_group_lanes(model, m, 0); }
+bool single_call_kernels_fit(const bf_fit_args &a) {
+    if (a.y_format != BF_Y_FLOAT32 || choose_lanes(a.model, a.m, a.group_lanes) == bf::kCtaLanes)
+        return false;
+    return a.p0 || a.m <= uint32_t(bf::group_guess_max_points());
+}
+int launch_single_call(const bf_fit_args &a, const bf_fit_outputs &out, float *guesses, unsigned long long *counter,
+                       int sms, cudaStream_t st) {
+    const int p = parameter_count(a.model);
+    const int lanes = choose_lanes(a.model, a.m, a.group_lanes);
+    bf::FitArgs f = make_args(a, p);
+    const long long n = (long long)a.n;
+    const float *p0 = a.p0;
+    if (!p0) {
+        BF_CUDA(bf::launch_guess(a.model, a.x, a.y, n, int(a.m), guesses, nullptr, sms, st, 0, nullptr));
+        p0 = guesses;
+    }
+    f.x = a.x;
+    f.y = a.y;
+    f.p0 = p0;
+    f.params = out.params;
+    f.status = out.status;
+    f.iterations = out.iterations;
+    f.chi2 = out.chi2;
+    f.covariance = out.covariance;
+    f.stderr_out = out.standard_errors;
+    f.ustatus = out.uncertainty_status;
+    f.n = n;
+    f.work_counter = counter;
+    BF_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+    bf::LaunchInfo info{};
+    BF_CUDA(bf::launch_fit(a.model, lanes, f, sms, st, &info, nullptr));
+    return BF_OK;
+}
 int report(int code, const std::string &message) { return fail(code, message); }
 int report_cuda(cudaError_t e, const char *what) { return cuda_fail(e, what); }
 } // namespace host

@@ -52,6 +52,15 @@ int prepare(const bf_fit_args *args, const bf_fit_outputs *out, FitArgs *base, i
 int prepare_segment(const bf_fit_args *args, const bf_fit_outputs *out, uint32_t max_points, FitArgs *base);
 // Group width the single-batch path picks for (model, M).
 int default_lanes(int model, uint32_t m);
+// Whether a fit call in device memory runs on the single-call group kernels
+// (float32 y, the group layout's M; a guess needs the shared-memory guess).
+bool single_call_kernels_fit(const bf_fit_args &dev_args);
+// Enqueue a validated fit call in device memory on `st` with the single-call
+// kernels (guess, LM, covariance), as bf_cuda_fit runs it: `guesses` holds N*P
+// floats when p0 is null, `counter` one work counter; grids for `sms` SMs' blocks.
+// Nothing is synchronised or timed.
+int launch_single_call(const bf_fit_args &dev_args, const bf_fit_outputs &dev_out, float *guesses,
+                       unsigned long long *counter, int sms, cudaStream_t st);
 int report(int code, const std::string &message);
 int report_cuda(cudaError_t e, const char *what);
 // Mixed batches (bf_batch.cu): plan, upload and run synchronously on stream[0].

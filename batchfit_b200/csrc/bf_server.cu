@@ -54,6 +54,8 @@ struct Request {
     size_t bytes = 0;           // device bytes charged to the budget
     char *block = nullptr;      // one device allocation for all of the request's buffers
     bf_batch_segment seg{};     // the request with device pointers
+    float *guesses = nullptr;   // N*P floats and a work counter: a large request alone
+    unsigned long long *counter = nullptr; // runs on the single-call kernels
     Clock::time_point submitted, done;
     int result = BF_OK;
     bool charged = false;   // its bytes count against the budget (admitted)
@@ -80,6 +82,7 @@ size_t request_bytes(const bf_fit_args &a) {
     if (a.uncertainties)
         b += align256(n * p * p * 4) + align256(n * p * 4);
     b += n * (2 * sizeof(bf::WorkItem) + p * 4);
+    b += align256(n * p * 4) + 256; // guesses and work counter of the single-call kernels
     return b;
 }
 
@@ -201,6 +204,8 @@ bool admit(bf_server *s) {
             o.standard_errors = reinterpret_cast<float *>(take(n * p * 4));
             o.uncertainty_status = reinterpret_cast<int32_t *>(take(n * 4));
         }
+        r->guesses = reinterpret_cast<float *>(take(n * p * 4));
+        r->counter = reinterpret_cast<unsigned long long *>(take(sizeof(unsigned long long)));
         r->seg.args = d;
         r->seg.out = o;
         e = cudaMemcpyAsync(const_cast<float *>(d.x), a.x, m * 4, cudaMemcpyHostToDevice, s->copy);
@@ -298,10 +303,22 @@ bool launch(bf_server *s, Slot &slot, bool allow_large) {
     // slot's blocks.
     const bool large = predicted > kBatchTargetMs;
     const bool shared = large && s->opt.max_in_flight != 1;
-    const int rc = bf::host::launch_planned(*slot.state, segs.data(), uint32_t(segs.size()),
-                                            s->opt.batch_flags | (shared ? BF_BATCH_NO_GRAPH : 0u),
-                                            shared ? s->sms * 3 / 4 : s->sms, slot.stream, &launched,
-                                            &slot.graph_used);
+    const int sms = shared ? s->sms * 3 / 4 : s->sms;
+    int rc = BF_OK;
+    const bool direct = large && take.size() == 1 && bf::host::single_call_kernels_fit(take[0]->seg.args);
+    if (direct) {
+        // A large request alone runs the single-call kernels (rows staged in shared
+        // memory, lanes per fit by (model, M)), as bf_cuda_fit would: faster per fit
+        // than the batch kernels.
+        const Request &r = *take[0];
+        rc = bf::host::launch_single_call(r.seg.args, r.seg.out, r.guesses, r.counter, sms, slot.stream);
+        slot.graph_used = false;
+        launched = false; // no batch timing events
+    } else {
+        rc = bf::host::launch_planned(*slot.state, segs.data(), uint32_t(segs.size()),
+                                      s->opt.batch_flags | (shared ? BF_BATCH_NO_GRAPH : 0u), sms, slot.stream,
+                                      &launched, &slot.graph_used);
+    }
     slot.launched = launched;
     if (rc != BF_OK) {
         // The batch could not be formed (a request failed validation on the device
@@ -322,7 +339,7 @@ bool launch(bf_server *s, Slot &slot, bool allow_large) {
     slot.requests = std::move(take);
     slot.busy = true;
     std::lock_guard<std::mutex> lock(s->mutex);
-    s->stats.batches += launched ? 1 : 0;
+    s->stats.batches += launched || direct ? 1 : 0;
     s->stats.max_batch_requests = std::max<uint64_t>(s->stats.max_batch_requests, slot.requests.size());
     return true;
 }

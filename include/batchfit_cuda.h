@@ -227,11 +227,14 @@ int bf_cuda_set_tuning(bf_cuda_context *ctx, const bf_tuning *in);
  * request predicted to take longer runs in a batch of its own, and smaller requests
  * that arrive after it may start before it.  At most one slot runs such a large
  * batch, launched with kernels sized for three quarters of the GPU's blocks, so
- * that short batches on the other slot always find room on every SM.  Outputs are
+ * that short batches on the other slot always find room on every SM; a large
+ * request alone runs on bf_cuda_fit's kernels (rows staged in shared memory) where
+ * its M allows.  Outputs are
  * copied into the request's host buffers, which stay owned by the caller and must
  * stay valid until the request completes.  A
- * request's result is the one bf_cuda_fit_batch gives for it; batch-mates only
- * change its lanes per fit (so results agree within the parity tolerances). */
+ * request's result is the one bf_cuda_fit_batch or bf_cuda_fit gives for it;
+ * batch-mates only change its lanes per fit (so results agree within the parity
+ * tolerances). */
 typedef struct bf_server bf_server;
 
 typedef struct bf_server_options {
@@ -245,7 +248,8 @@ typedef struct bf_server_stats {
     uint64_t submitted, completed, failed, fits_completed, batches;
     uint64_t memory_in_use, memory_peak, memory_budget; /* bytes charged to admitted requests */
     uint64_t max_batch_requests;                        /* most requests in one launch */
-    double gpu_ms;                                      /* summed device time of the batches */
+    double gpu_ms;                                      /* summed device time of the mixed batches (not of
+                                                           large requests run alone on the single-call kernels) */
 } bf_server_stats;
 
 int bf_server_create(int device, const bf_server_options *options, bf_server **out);
