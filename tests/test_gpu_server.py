@@ -171,3 +171,36 @@ def test_allocation_failure_and_cancellation_leave_the_others_intact(bf):
         alone = bf.fit_batch([r])[0]
         a, w, n = same_within_tolerance(r, got, alone)
         assert a >= 0.99 and w >= 0.99
+
+
+def test_large_request_alone_equals_the_single_call(bf):
+    """A request predicted to take longer than a short batch runs alone on
+    bf_cuda_fit's kernels (grids for three quarters of the SMs): its results equal
+    a plain fit of the same data bit for bit, with a short request served beside it."""
+    big = make_requests(1, seed=21, n_max=2)[0]
+    rng = np.random.default_rng(22)
+    n, m = 80000, 1024
+    x = np.linspace(-10, 10, m).astype(np.float32)
+    a = rng.uniform(0.5, 5.0, n)[:, None]
+    c = rng.uniform(-6, 6, n)[:, None]
+    w = np.exp(rng.uniform(np.log(0.1), np.log(3.0), n))[:, None]
+    eta = rng.uniform(0, 1, n)[:, None]
+    z = (x - c) / w
+    y = (a * ((1 - eta) * np.exp(-4 * np.log(2) * z * z) + eta / (1 + 4 * z * z))
+         + 0.01 * a * rng.normal(size=(n, m))).astype(np.float32)
+    lo, hi = W.MIXED_BOUNDS["pseudo_voigt"]
+    bounds = (np.array(lo, np.float32), np.array(hi, np.float32))
+    with bf.Server() as server:
+        t_big = server.submit(x, y, "pseudo_voigt", None, bounds, uncertainties=True)
+        t_small = server.submit(big["x"], big["y"], big["model"], None, big["bounds"], uncertainties=False)
+        got, small = t_big.result(), t_small.result()
+        st = server.stats()
+    assert st["failed"] == 0 and st["memory_in_use"] == 0
+    ref = bf.fit(x, y, "pseudo_voigt", None, bounds, "cuda", uncertainties=True)
+    for k in ("params", "status", "iterations", "chi2", "covariance", "stderr", "uncertainty_status"):
+        want = getattr(ref, k)
+        want = want.cpu().numpy() if hasattr(want, "cpu") else np.asarray(want)
+        np.testing.assert_array_equal(np.asarray(getattr(got, k)), want, err_msg=k)
+    alone = bf.fit_batch([dict(big, uncertainties=False)])[0]
+    a_, w_, _ = same_within_tolerance(big, small, alone)
+    assert a_ == 1.0 and w_ >= 0.99
