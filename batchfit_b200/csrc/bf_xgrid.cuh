@@ -15,6 +15,9 @@ __device__ __forceinline__ XConst xconst_warp(const float *x, int m) {
     unsigned min_abs = 0x7f800000u, min_diff = 0x7f800000u;
     bool fin = true, up = true, down = true, strict = true, varied = false;
     const float x0 = __ldg(x);
+    // Unrolled so that the loads of several iterations are in flight together (the
+    // loop is latency-bound on them otherwise: one warp per segment, M/32 rounds).
+#pragma unroll 8
     for (int j = int(lane); j < m; j += 32) {
         const float v = __ldg(x + j);
         fin = fin && isfinite(v);
