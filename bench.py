@@ -43,10 +43,10 @@ MODEL, M, P = "pseudo_voigt", 512, 4
 WORKLOAD = "pseudo_voigt_plain: 1M pseudo-Voigt fits, M=512, float32, p0=None, uncertainties=True"
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) of the LM kernel per fit, from the committed ncu capture
-# of the same kernel on 100,000 fits (profiles/fit_kernels_pv512_100k.md): 206.48 MB
-# read + 5.33 MB written.  Traffic grows with the fits processed, so the bench scales
+# of the same kernel on 100,000 fits (profiles/fit_kernels_pv512_100k.md): 206.46 MB
+# read + 4.45 MB written.  Traffic grows with the fits processed, so the bench scales
 # it to the launch's fit count.
-TRAFFIC_BYTES_PER_FIT = (206.481408e6 + 5.333248e6) / 100_000
+TRAFFIC_BYTES_PER_FIT = (206.462464e6 + 4.445696e6) / 100_000
 
 
 def parse():
