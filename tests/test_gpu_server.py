@@ -204,3 +204,12 @@ def test_large_request_alone_equals_the_single_call(bf):
     alone = bf.fit_batch([dict(big, uncertainties=False)])[0]
     a_, w_, _ = same_within_tolerance(big, small, alone)
     assert a_ == 1.0 and w_ >= 0.99
+    # With initial values given (no guess kernel): again the single call's results.
+    p0 = np.where(np.isfinite(got.params), got.params, 1.0).astype(np.float32)
+    with bf.Server() as server:
+        got0 = server.submit(x, y, "pseudo_voigt", p0, bounds, uncertainties=False).result()
+    ref0 = bf.fit(x, y, "pseudo_voigt", p0, bounds, "cuda")
+    for k in ("params", "status", "iterations", "chi2"):
+        want = getattr(ref0, k)
+        want = want.cpu().numpy() if hasattr(want, "cpu") else np.asarray(want)
+        np.testing.assert_array_equal(np.asarray(getattr(got0, k)), want, err_msg=k)
