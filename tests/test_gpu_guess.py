@@ -31,7 +31,7 @@ def test_guess_pseudo_voigt_plain(bf, oracle):
 
 
 @pytest.mark.parametrize("model", ["gaussian", "lorentzian", "pseudo_voigt", "two_lorentzian"])
-@pytest.mark.parametrize("m", [5, 7, 33, 64, 129, 300, 1024])
+@pytest.mark.parametrize("m", [5, 7, 33, 64, 129, 300, 701, 1024, 1601, 2603])
 def test_guess_random_shapes(bf, oracle, model, m):
     rng = np.random.default_rng(1000 + m)
     n = 257
